@@ -1,0 +1,92 @@
+"""Pins the CPU oracle to outputs of the reference simulator's own CPU algorithm.
+
+The fixtures were produced by ``tests/golden/make_golden.py`` from the reference's
+``src/MPO.py`` / ``src/summary.py`` (complex64), so the tolerance is 1e-5 relative.
+"""
+import glob
+import os
+from collections import defaultdict
+
+import numpy as np
+import pytest
+
+from oracle import fock, mpo
+
+TOL = 1e-5
+
+
+def _cases(golden_dir):
+    return sorted(glob.glob(os.path.join(golden_dir, "ref_n*.npz")))
+
+
+def _bond_spectrum(lam, charge, d):
+    """Sorted (charge, value) multiset of a bond's non-zero Lambda."""
+    out = defaultdict(list)
+    for v, c in zip(lam, charge):
+        if v > 0 and c[0] < d:
+            out[(int(c[0]), int(c[1]))].append(float(v))
+    return {k: np.sort(np.array(v))[::-1] for k, v in out.items()}
+
+
+def _assert_spectra_close(a, b, scale):
+    keys = set(a) | set(b)
+    for k in keys:
+        x, y = a.get(k, np.zeros(0)), b.get(k, np.zeros(0))
+        n = max(len(x), len(y))
+        x = np.pad(x, (0, n - len(x)))
+        y = np.pad(y, (0, n - len(y)))
+        np.testing.assert_allclose(x, y, rtol=0, atol=TOL * scale, err_msg=str(k))
+
+
+def test_bs_tensors_match_reference(golden_dir):
+    fx = np.load(os.path.join(golden_dir, "ref_bs_tensors.npz"))
+    for key in fx.files:
+        _, seed, d, r = key.split("_")
+        U4 = fx[key]
+        U3 = fock.reference_random_tensor(int(seed), int(d), float(r.replace("p", ".")))
+        np.testing.assert_allclose(fock.tensor3_to_4(U3), U4, atol=2e-6)
+
+
+@pytest.mark.parametrize("path", _cases(os.path.join(os.path.dirname(__file__), "golden")),
+                         ids=lambda p: os.path.basename(p)[:-4])
+def test_oracle_matches_reference(path):
+    fx = np.load(path)
+    n, n_in, d, chi = int(fx["n"]), int(fx["n_in"]), int(fx["d"]), int(fx["chi"])
+    eta = 1.0 - float(fx["loss"])
+    st = mpo.initial_state(n, range(n_in), eta, d, chi)
+    # initial state: Lambda spectra per bond and trace
+    il, ic = fx["init_lambda"], fx["init_charge"]
+    for b in range(1, n):
+        _assert_spectra_close(_bond_spectrum(st.Lambda[b - 1], st.charge[b], d),
+                              _bond_spectrum(il[b - 1], ic[b], d), 1.0)
+    assert abs(mpo.trace(st).real - fx["init_trace"]) < TOL
+    # BS by BS: per-sector singular values, matched by centre charge.  The reference
+    # (complex64) keeps singular values at its ~1e-8 noise floor as extra bond entries,
+    # so sector shapes may differ; spectra are compared zero-padded, normwise.
+    pos = 0
+    sig = fx["sigma"]
+    offs = np.concatenate([[0], np.cumsum(fx["sigma_len"])])
+    for t, (mode, seed, r) in enumerate(zip(fx["bs_mode"], fx["bs_seed"], fx["bs_refl"])):
+        info = mpo.bs_update(st, int(mode), fock.reference_random_tensor(int(seed), d, float(r)))
+        ns = int(fx["sectors_per_bs"][t])
+        ref_s = {}
+        for s in range(ns):
+            ref_s[tuple(int(x) for x in fx["sector_id"][pos])] = sig[offs[pos]:offs[pos + 1]]
+            pos += 1
+        mine_s = {tuple(sec): sv for sec, sv in zip(info.sectors, info.sigma)}
+        scale = max([float(v.max()) for v in ref_s.values() if len(v)] + [1e-30])
+        for sec in set(ref_s) | set(mine_s):
+            a = np.sort(ref_s.get(sec, np.zeros(0)))[::-1]
+            b = np.sort(mine_s.get(sec, np.zeros(0)))[::-1]
+            m = max(len(a), len(b))
+            np.testing.assert_allclose(np.pad(b, (0, m - len(b))), np.pad(a, (0, m - len(a))),
+                                       rtol=0, atol=TOL * scale, err_msg="bs %d sector %s" % (t, sec))
+    # final state
+    fl, fc = fx["final_lambda"], fx["final_charge"]
+    for b in range(1, n):
+        _assert_spectra_close(_bond_spectrum(st.Lambda[b - 1], st.charge[b], d),
+                              _bond_spectrum(fl[b - 1], fc[b], d), 1.0)
+    assert abs(mpo.trace(st).real - fx["final_trace"]) < TOL
+    P = mpo.marginals(st).real
+    np.testing.assert_allclose(P, fx["final_marginals"], atol=TOL)
+    np.testing.assert_allclose(mpo.entanglement_entropy(st), fx["final_ee"], atol=1e-4)
