@@ -1,0 +1,830 @@
+// libbsmpo C ABI and host orchestration of the beam-splitter MPO update.
+//
+// The host keeps a mirror of the per-bond charge-block sizes (they change only when
+// an update writes a new bond, and the update reports its kept counts), so every
+// launch of an update is planned on the host without reading device data; the one
+// device->host synchronisation per update reads the kept counts after selection.
+//
+// Per update (bond layout of src/MPO.py:158-303, GPU driver
+// src/beam_splitter_parallel/Rank.py:32-206):
+//   Theta grouped GEMM -> gate mix (C per sector and the Jacobi matrix) ->
+//   blocked one-sided Jacobi rounds -> column norms + sort -> top-chi selection ->
+//   [sync: kept counts] -> V extraction -> W = V^H C grouped GEMM -> scatter.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/bsmpo.h"
+#include "common.cuh"
+#include "kernels.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+constexpr int MAX_SWEEPS = 40;
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+struct HostStage {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace
+
+struct bsmpo_ctx {
+  int n = 0, d = 0, chi = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  double cutoff = 0.0;
+  // device state
+  cplx* gamma = nullptr;     // [n][chi][chi]
+  double* lam = nullptr;     // [n+1][chi]  (edges: 1 on occupied slots)
+  int* charge = nullptr;     // [n+1][chi][2]
+  bool loaded = false;
+  // host mirror of block sizes: cnt[b * d*d + c0*d + c1]
+  std::vector<int> cnt;
+  // workspaces
+  DevBuf theta, cbuf, abuf, wbuf, vbuf, sig, keys, perm, tab, tab2, rot, kept, u3, m4, env_l,
+      env_r, part, outv, dims;
+  HostStage stage, stage2, hres;
+  // last update diagnostics (host)
+  std::vector<int> last_cc, last_shape, last_kept, last_k;
+  std::vector<int64_t> last_soff;
+  double last_trunc = 0.0, last_gemm = 0.0, last_svd = 0.0, last_bytes = 0.0;
+  int last_sweeps = 0;
+  int last_ns = 0;
+  int64_t launches = 0;
+  std::string err;
+};
+
+namespace {
+
+int fail(bsmpo_ctx* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  g_last_error = msg;
+  return code;
+}
+
+#define CK(h, call)                                                                    \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail((h), BSMPO_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define CKL(h, call)            \
+  do {                          \
+    CK(h, call);                \
+    (h)->launches++;            \
+  } while (0)
+
+int grow(bsmpo_ctx* h, DevBuf& b, size_t bytes) {
+  if (bytes <= b.bytes) return BSMPO_OK;
+  // the stream may still use the old buffer
+  CK(h, cudaStreamSynchronize(h->stream));
+  if (b.p) CK(h, cudaFree(b.p));
+  b.p = nullptr;
+  b.bytes = 0;
+  size_t want = align_up(bytes + bytes / 4 + 256, 256);
+  if (cudaMalloc(&b.p, want) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(h, BSMPO_ENOMEM, "device allocation of " + std::to_string(want) + " bytes failed");
+  }
+  b.bytes = want;
+  return BSMPO_OK;
+}
+
+int grow_host(bsmpo_ctx* h, HostStage& b, size_t bytes) {
+  if (bytes <= b.bytes) return BSMPO_OK;
+  CK(h, cudaStreamSynchronize(h->stream));
+  if (b.p) CK(h, cudaFreeHost(b.p));
+  b.p = nullptr;
+  b.bytes = 0;
+  size_t want = align_up(bytes + bytes / 4 + 256, 256);
+  CK(h, cudaMallocHost(&b.p, want));
+  b.bytes = want;
+  return BSMPO_OK;
+}
+
+// offsets of the lexicographic charge blocks of one bond (d*d + 1 entries)
+void block_offsets(const int* cnt, int d, int* off) {
+  off[0] = 0;
+  for (int q = 0; q < d * d; ++q) off[q + 1] = off[q] + cnt[q];
+}
+
+struct Plan {
+  UpdateTables tab;
+  std::vector<int> tidx;
+  std::vector<ThetaDesc> td;
+  std::vector<SectorDesc> sd;
+  std::vector<MixPair> pairs;
+  std::vector<GemmGroup> gg;
+  std::vector<JacobiWork> jw;
+  int mix_tiles = 0, gemm_tiles = 0, jac_ctas = 0, max_rounds = 0, max_k = 0, max_left_m2 = 0;
+  int64_t theta_elems = 0, c_elems = 0, a_elems = 0, s_elems = 0, w_elems = 0, v_elems = 0;
+  double flops_theta = 0.0;
+};
+
+int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
+  const int d = h->d, dd = d * d;
+  const int* cL = &h->cnt[(size_t)mode * dd];
+  const int* cC = &h->cnt[(size_t)(mode + 1) * dd];
+  const int* cR = &h->cnt[(size_t)(mode + 2) * dd];
+  UpdateTables& T = P.tab;
+  std::memset(&T, 0, sizeof(T));
+  T.d = d;
+  T.chi = h->chi;
+  T.mode = mode;
+  block_offsets(cL, d, T.offL);
+  block_offsets(cC, d, T.offC);
+  block_offsets(cR, d, T.offR);
+  for (int i = 0; i < BSMPO_MAX_Q; ++i) { T.sidx[i] = -1; T.pair_of[i] = -1; }
+  // sector range: the reference loop (src/MPO.py:191-206) over occupied charges
+  int hi0 = -1, hi1 = -1, lo0 = d, lo1 = d;
+  for (int a0 = 0; a0 < d; ++a0)
+    for (int a1 = 0; a1 < d; ++a1) {
+      if (cL[a0 * d + a1] > 0) { hi0 = std::max(hi0, a0); hi1 = std::max(hi1, a1); }
+      if (cR[a0 * d + a1] > 0) { lo0 = std::min(lo0, a0); lo1 = std::min(lo1, a1); }
+    }
+  auto rows_of = [&](int a0, int from1) { return T.offL[(a0 + 1) * d] - T.offL[a0 * d + from1]; };
+  auto cols_of = [&](int b0, int to1) { return T.offR[b0 * d + to1 + 1] - T.offR[b0 * d]; };
+  P.sd.clear();
+  int64_t c_off = 0, a_off = 0, s_off = 0, w_off = 0, v_off = 0;
+  for (int cc0 = lo0; cc0 <= hi0; ++cc0)
+    for (int cc1 = lo1; cc1 <= hi1; ++cc1) {
+      SectorDesc S;
+      std::memset(&S, 0, sizeof(S));
+      S.cc0 = cc0;
+      S.cc1 = cc1;
+      int m = 0, n = 0;
+      for (int a0 = cc0; a0 < d; ++a0) { S.row_start[a0] = m; m += rows_of(a0, cc1); }
+      for (int b0 = 0; b0 <= cc0; ++b0) { S.col_start[b0] = n; n += cols_of(b0, cc1); }
+      if (m == 0 || n == 0) continue;
+      S.m = m;
+      S.n = n;
+      S.left = m < n ? 1 : 0;
+      S.k = S.left ? m : n;
+      S.rows_g = S.left ? n : m;
+      S.rows_tot = S.left ? n + m : m;
+      S.c_off = c_off; c_off += (int64_t)m * n;
+      S.a_off = a_off; a_off += (int64_t)S.rows_tot * S.k;
+      S.s_off = s_off; s_off += S.k;
+      S.w_off = w_off; w_off += (int64_t)S.k * n;
+      S.v_off = v_off; v_off += (int64_t)m * S.k;
+      T.sidx[cc0 * d + cc1] = (int)P.sd.size();
+      P.sd.push_back(S);
+    }
+  const int ns = (int)P.sd.size();
+  if (ns > BSMPO_MAX_Q) return fail(h, BSMPO_EINVAL, "too many sectors");
+  for (int s = 0; s < ns; ++s) {
+    const int p = T.sidx[P.sd[s].cc1 * d + P.sd[s].cc0];
+    T.pair_of[s] = p;
+  }
+  T.n_sectors = ns;
+  P.c_elems = c_off; P.a_elems = a_off; P.s_elems = s_off; P.w_elems = w_off; P.v_elems = v_off;
+  // Theta groups (q, a0, b0)
+  P.tidx.assign((size_t)dd * d * d, -1);
+  P.td.clear();
+  P.gg.clear();
+  int64_t t_off = 0;
+  int tiles = 0;
+  const int TMt = zgemm_tile_m(), TNt = zgemm_tile_n();
+  const int64_t chi2 = (int64_t)h->chi * h->chi;
+  P.flops_theta = 0.0;
+  for (int q0 = 0; q0 < d; ++q0)
+    for (int q1 = 0; q1 < d; ++q1) {
+      const int nk = cC[q0 * d + q1];
+      if (nk == 0) continue;
+      for (int a0 = q0; a0 < d; ++a0) {
+        const int nrow = rows_of(a0, q1);
+        if (nrow == 0) continue;
+        for (int b0 = 0; b0 <= q0; ++b0) {
+          const int ncol = cols_of(b0, q1);
+          if (ncol == 0) continue;
+          ThetaDesc D;
+          D.q0 = q0; D.q1 = q1; D.a0 = a0; D.b0 = b0;
+          D.row0 = T.offL[a0 * d + q1]; D.nrow = nrow;
+          D.col0 = T.offR[b0 * d]; D.ncol = ncol;
+          D.k0 = T.offC[q0 * d + q1]; D.nk = nk;
+          D.off = t_off;
+          t_off += (int64_t)nrow * ncol;
+          P.tidx[((q0 * d + q1) * d + a0) * d + b0] = (int)P.td.size();
+          P.td.push_back(D);
+          GemmGroup g;
+          std::memset(&g, 0, sizeof(g));
+          g.M = nrow; g.N = ncol; g.K = nk;
+          g.lda = h->chi; g.ldb = h->chi; g.ldc = ncol;
+          g.opA = 0; g.opB = 0; g.beta = 0;
+          g.tiles_n = ceil_div(ncol, TNt);
+          g.tile_start = tiles;
+          tiles += ceil_div(nrow, TMt) * g.tiles_n;
+          g.a_off = (int64_t)mode * chi2 + (int64_t)D.row0 * h->chi + D.k0;
+          g.b_off = (int64_t)(mode + 1) * chi2 + (int64_t)D.k0 * h->chi + D.col0;
+          g.c_off = D.off;
+          g.ks_off = g.rs_off = g.cs_off = -1;
+          P.gg.push_back(g);
+          P.flops_theta += 8.0 * nrow * (double)nk * ncol;
+        }
+      }
+    }
+  P.theta_elems = t_off;
+  P.gemm_tiles = tiles;
+  T.n_theta = (int)P.td.size();
+  // mix pairs (a >= b)
+  P.pairs.clear();
+  int mt = 0;
+  for (int a0 = 0; a0 < d; ++a0)
+    for (int a1 = 0; a1 < d; ++a1) {
+      const int na = cL[a0 * d + a1];
+      if (!na) continue;
+      for (int b0 = 0; b0 <= a0; ++b0)
+        for (int b1 = 0; b1 <= a1; ++b1) {
+          const int nb = cR[b0 * d + b1];
+          if (!nb) continue;
+          MixPair M;
+          M.a0 = a0; M.a1 = a1; M.b0 = b0; M.b1 = b1;
+          M.row0 = T.offL[a0 * d + a1]; M.nrow = na;
+          M.col0 = T.offR[b0 * d + b1]; M.ncol = nb;
+          M.tile_start = mt;
+          M.pad_ = 0;
+          mt += ceil_div(na * nb, 256);
+          P.pairs.push_back(M);
+        }
+    }
+  P.mix_tiles = mt;
+  T.n_pairs = (int)P.pairs.size();
+  // Jacobi work
+  P.jw.clear();
+  int ctas = 0;
+  P.max_rounds = 0;
+  P.max_k = 0;
+  P.max_left_m2 = 0;
+  const int JBc = jacobi_block_cols();
+  for (int s = 0; s < ns; ++s) {
+    const SectorDesc& S = P.sd[s];
+    P.max_k = std::max(P.max_k, S.k);
+    if (S.left) P.max_left_m2 = std::max(P.max_left_m2, S.m * S.m);
+    JacobiWork w;
+    w.sector = s;
+    w.nblk = ceil_div(S.k, JBc);
+    const int nbp = w.nblk + (w.nblk & 1);
+    w.npairs = nbp / 2;
+    w.rounds = nbp - 1;
+    w.cta_start = ctas;
+    w.pad_ = 0;
+    ctas += w.npairs;
+    P.max_rounds = std::max(P.max_rounds, w.rounds);
+    P.jw.push_back(w);
+  }
+  P.jac_ctas = ctas;
+  return BSMPO_OK;
+}
+
+// packs plan tables into the pinned stage and copies them to the device table buffer
+struct TabLayout {
+  size_t tab, tidx, td, sd, pairs, gg, jw, total;
+};
+
+TabLayout layout_of(const Plan& P) {
+  TabLayout L;
+  size_t o = 0;
+  L.tab = o; o = align_up(o + sizeof(UpdateTables), 256);
+  L.tidx = o; o = align_up(o + P.tidx.size() * sizeof(int), 256);
+  L.td = o; o = align_up(o + P.td.size() * sizeof(ThetaDesc) + 1, 256);
+  L.sd = o; o = align_up(o + P.sd.size() * sizeof(SectorDesc) + 1, 256);
+  L.pairs = o; o = align_up(o + P.pairs.size() * sizeof(MixPair) + 1, 256);
+  L.gg = o; o = align_up(o + P.gg.size() * sizeof(GemmGroup) + 1, 256);
+  L.jw = o; o = align_up(o + P.jw.size() * sizeof(JacobiWork) + 1, 256);
+  L.total = o;
+  return L;
+}
+
+template <typename T>
+void put(void* base, size_t off, const std::vector<T>& v) {
+  if (!v.empty()) std::memcpy(static_cast<char*>(base) + off, v.data(), v.size() * sizeof(T));
+}
+
+int check_mode(bsmpo_ctx* h, int mode) {
+  if (!h) return fail(nullptr, BSMPO_EINVAL, "null handle");
+  if (!h->loaded) return fail(h, BSMPO_EINVAL, "no state loaded");
+  if (mode < 0 || mode > h->n - 2) return fail(h, BSMPO_EINVAL, "mode out of range");
+  return BSMPO_OK;
+}
+
+int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
+  int rc = check_mode(h, mode);
+  if (rc) return rc;
+  const int d = h->d, chi = h->chi, dd = d * d;
+  cudaStream_t st = h->stream;
+  Plan P;
+  if ((rc = make_plan(h, mode, P))) return rc;
+  const int ns = (int)P.sd.size();
+  h->last_ns = ns;
+  if (ns == 0) return fail(h, BSMPO_EINVAL, "update with an empty left or right bond");
+  // workspaces
+  if ((rc = grow(h, h->theta, std::max<int64_t>(P.theta_elems, 1) * sizeof(cplx)))) return rc;
+  if ((rc = grow(h, h->cbuf, std::max<int64_t>(P.c_elems, 1) * sizeof(cplx)))) return rc;
+  if ((rc = grow(h, h->abuf, std::max<int64_t>(P.a_elems, 1) * sizeof(cplx)))) return rc;
+  if ((rc = grow(h, h->wbuf, std::max<int64_t>(P.w_elems, 1) * sizeof(cplx)))) return rc;
+  if ((rc = grow(h, h->vbuf, std::max<int64_t>(P.v_elems, 1) * sizeof(cplx)))) return rc;
+  if ((rc = grow(h, h->sig, std::max<int64_t>(P.s_elems, 1) * sizeof(double)))) return rc;
+  if ((rc = grow(h, h->keys, std::max<int64_t>(P.s_elems, 1) * sizeof(double)))) return rc;
+  if ((rc = grow(h, h->perm, std::max<int64_t>(P.s_elems, 1) * sizeof(int)))) return rc;
+  if ((rc = grow(h, h->rot, (size_t)3 * ns * sizeof(int)))) return rc;
+  if ((rc = grow(h, h->kept, (size_t)(ns + 1) * sizeof(int) + 64))) return rc;
+  const TabLayout L = layout_of(P);
+  if ((rc = grow(h, h->tab, L.total))) return rc;
+  if ((rc = grow_host(h, h->stage, L.total))) return rc;
+  if ((rc = grow_host(h, h->hres, 4096 + (size_t)(ns + 2) * sizeof(int) + 3 * ns * sizeof(int)))) return rc;
+  char* hs = static_cast<char*>(h->stage.p);
+  std::memcpy(hs + L.tab, &P.tab, sizeof(UpdateTables));
+  put(hs, L.tidx, P.tidx);
+  put(hs, L.td, P.td);
+  put(hs, L.sd, P.sd);
+  put(hs, L.pairs, P.pairs);
+  put(hs, L.gg, P.gg);
+  put(hs, L.jw, P.jw);
+  char* dt = static_cast<char*>(h->tab.p);
+  CK(h, cudaMemcpyAsync(dt, hs, L.total, cudaMemcpyHostToDevice, st));
+  const UpdateTables* tab_d = reinterpret_cast<const UpdateTables*>(dt + L.tab);
+  const int* tidx_d = reinterpret_cast<const int*>(dt + L.tidx);
+  const ThetaDesc* td_d = reinterpret_cast<const ThetaDesc*>(dt + L.td);
+  SectorDesc* sd_d = reinterpret_cast<SectorDesc*>(dt + L.sd);
+  const MixPair* pairs_d = reinterpret_cast<const MixPair*>(dt + L.pairs);
+  const GemmGroup* gg_d = reinterpret_cast<const GemmGroup*>(dt + L.gg);
+  const JacobiWork* jw_d = reinterpret_cast<const JacobiWork*>(dt + L.jw);
+  const int64_t chi2 = (int64_t)chi * chi;
+
+  // 1. Theta_q = Glc[a, q] Gcr[q, b] for every valid triple
+  CKL(h, launch_zgemm_grouped(h->gamma, h->gamma, h->theta.p, nullptr, gg_d, (int)P.gg.size(),
+                              P.gemm_tiles, st));
+  // 2. identity rows of [T^H; I] and the gate mix
+  CKL(h, launch_identity_rows(sd_d, ns, P.max_left_m2, h->abuf.p, st));
+  CKL(h, launch_mix_d(d, tab_d, tidx_d, td_d, sd_d, pairs_d, (int)P.pairs.size(), P.mix_tiles,
+                      u3_dev, h->theta.p, h->lam + (size_t)(mode + 2) * chi, h->cbuf.p, h->abuf.p,
+                      st));
+  // 3. blocked one-sided Jacobi
+  CK(h, cudaMemsetAsync(h->rot.p, 0, (size_t)3 * ns * sizeof(int), st));
+  int* hrot = reinterpret_cast<int*>(static_cast<char*>(h->hres.p) + 1024);
+  int t = 0;
+  const int t_max = MAX_SWEEPS * std::max(1, P.max_rounds);
+  int min_rounds = P.max_rounds;
+  for (const auto& w : P.jw) min_rounds = std::min(min_rounds, w.rounds);
+  bool converged = false;
+  int checks = 0;
+  while (t < t_max) {
+    // run one sweep of the largest sector, then test convergence
+    const int chunk = std::max(1, P.max_rounds);
+    for (int i = 0; i < chunk && t < t_max; ++i, ++t) {
+      // tol <= 0: per-sector default 4 eps sqrt(rows of the Gram), at least 8 eps
+      CKL(h, launch_jacobi_round(sd_d, jw_d, (int)P.jw.size(), P.jac_ctas, t, h->abuf.p,
+                                 reinterpret_cast<int*>(h->rot.p), 0.0, MAX_SWEEPS, st));
+    }
+    CK(h, cudaMemcpyAsync(hrot, h->rot.p, (size_t)3 * ns * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(h, cudaStreamSynchronize(st));
+    ++checks;
+    bool all = true;
+    for (int s = 0; s < ns; ++s) {
+      const int R = P.jw[s].rounds;
+      const int done = t / R;
+      if (done < 1 || hrot[3 * s + (done - 1) % 3] != 0) { all = false; break; }
+    }
+    if (all) { converged = true; break; }
+  }
+  h->last_sweeps = t / std::max(1, P.max_rounds);
+  if (!converged) return fail(h, BSMPO_ECONVERGE, "Jacobi SVD did not converge");
+  CKL(h, launch_jacobi_finish(sd_d, ns, P.max_k, h->abuf.p, reinterpret_cast<double*>(h->sig.p),
+                              reinterpret_cast<int*>(h->perm.p), st));
+  // 4. selection -> kept counts (the one host sync of the update)
+  int* kept_d = reinterpret_cast<int*>(h->kept.p);
+  double* trunc_d = reinterpret_cast<double*>(static_cast<char*>(h->kept.p) +
+                                              align_up((size_t)(ns + 1) * sizeof(int), 16));
+  CKL(h, launch_select(tab_d, sd_d, ns, reinterpret_cast<double*>(h->sig.p),
+                       reinterpret_cast<double*>(h->keys.p), h->cutoff, chi, kept_d, trunc_d, st));
+  int* hk = reinterpret_cast<int*>(h->hres.p);
+  double* htw = reinterpret_cast<double*>(static_cast<char*>(h->hres.p) + 512);
+  CK(h, cudaMemcpyAsync(hk, kept_d, (size_t)(ns + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(h, cudaMemcpyAsync(htw, trunc_d, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(h, cudaStreamSynchronize(st));
+  const int total_kept = hk[ns];
+  // 5. V and W = V^H C
+  std::vector<GemmGroup> wg;
+  int wtiles = 0, max_vm = 0;
+  double flops_w = 0.0;
+  const int TMt = zgemm_tile_m(), TNt = zgemm_tile_n();
+  for (int s = 0; s < ns; ++s) {
+    const SectorDesc& S = P.sd[s];
+    const int kp = hk[s];
+    max_vm = std::max(max_vm, kp * S.m);
+    if (kp == 0) continue;
+    GemmGroup g;
+    std::memset(&g, 0, sizeof(g));
+    g.M = kp; g.N = S.n; g.K = S.m;
+    g.lda = kp; g.ldb = S.n; g.ldc = S.n;
+    g.opA = 1; g.opB = 0; g.beta = 0;
+    g.tiles_n = ceil_div(S.n, TNt);
+    g.tile_start = wtiles;
+    wtiles += ceil_div(kp, TMt) * g.tiles_n;
+    g.a_off = S.v_off; g.b_off = S.c_off; g.c_off = S.w_off;
+    g.ks_off = g.rs_off = g.cs_off = -1;
+    wg.push_back(g);
+    flops_w += 8.0 * kp * (double)S.m * S.n;
+  }
+  const size_t wbytes = align_up(wg.size() * sizeof(GemmGroup) + 1, 256);
+  if ((rc = grow(h, h->tab2, wbytes))) return rc;
+  if ((rc = grow_host(h, h->stage2, wbytes))) return rc;
+  put(h->stage2.p, 0, wg);
+  CK(h, cudaMemcpyAsync(h->tab2.p, h->stage2.p, wbytes, cudaMemcpyHostToDevice, st));
+  CKL(h, launch_extract_v(sd_d, ns, max_vm, h->abuf.p, reinterpret_cast<double*>(h->sig.p),
+                          reinterpret_cast<int*>(h->perm.p), h->vbuf.p, st));
+  CKL(h, launch_zgemm_grouped(h->vbuf.p, h->cbuf.p, h->wbuf.p, nullptr,
+                              reinterpret_cast<const GemmGroup*>(h->tab2.p), (int)wg.size(), wtiles,
+                              st));
+  // 6. scatter into Gamma[mode], Gamma[mode+1], Lambda / charge of bond mode+1
+  CKL(h, launch_scatter(tab_d, sd_d, ns, total_kept, chi, h->charge + (size_t)mode * chi * 2,
+                        h->charge + (size_t)(mode + 2) * chi * 2, h->vbuf.p, h->wbuf.p,
+                        reinterpret_cast<double*>(h->sig.p), h->gamma + (size_t)mode * chi2,
+                        h->gamma + (size_t)(mode + 1) * chi2, h->lam + (size_t)(mode + 1) * chi,
+                        h->charge + (size_t)(mode + 1) * chi * 2, st));
+  // algorithmic minimum bytes: read Glc, Gcr, write Gamma_L, Gamma_R (complex128)
+  {
+    double nl = 0, nc = 0, nr = 0;
+    for (int q = 0; q < dd; ++q) {
+      nl += h->cnt[(size_t)mode * dd + q];
+      nc += h->cnt[(size_t)(mode + 1) * dd + q];
+      nr += h->cnt[(size_t)(mode + 2) * dd + q];
+    }
+    h->last_bytes = 16.0 * (nl * nc + nc * nr + ((double)nl + nr) * total_kept);
+  }
+  // host mirror and diagnostics
+  int* cM = &h->cnt[(size_t)(mode + 1) * dd];
+  std::fill(cM, cM + dd, 0);
+  h->last_cc.assign(2 * ns, 0);
+  h->last_shape.assign(2 * ns, 0);
+  h->last_kept.assign(ns, 0);
+  h->last_k.assign(ns, 0);
+  h->last_soff.assign(ns, 0);
+  double svd_flops = 0.0;
+  for (int s = 0; s < ns; ++s) {
+    const SectorDesc& S = P.sd[s];
+    cM[S.cc0 * d + S.cc1] = hk[s];
+    h->last_cc[2 * s] = S.cc0;
+    h->last_cc[2 * s + 1] = S.cc1;
+    h->last_shape[2 * s] = S.m;
+    h->last_shape[2 * s + 1] = S.n;
+    h->last_kept[s] = hk[s];
+    h->last_k[s] = S.k;
+    h->last_soff[s] = S.s_off;
+    // one sweep: every column pair's Gram (rows_g) and rotation (rows_tot), 8 flops / complex MAC
+    svd_flops += 4.0 * (double)S.k * S.k * (S.rows_g + S.rows_tot);
+  }
+  h->last_trunc = *htw;
+  h->last_gemm = P.flops_theta + flops_w;
+  h->last_svd = svd_flops * h->last_sweeps;
+  (void)checks;
+  return BSMPO_OK;
+}
+
+M8 transpose_to_m8(const double* S) {
+  // S = [[s00, s01], [s10, s11]] acting on the state -> tensor of M = S^T
+  M8 m;
+  m.v[0] = S[0]; m.v[1] = S[1];   // M00 = S00
+  m.v[2] = S[4]; m.v[3] = S[5];   // M01 = S10
+  m.v[4] = S[2]; m.v[5] = S[3];   // M10 = S01
+  m.v[6] = S[6]; m.v[7] = S[7];   // M11 = S11
+  return m;
+}
+
+int env_all(bsmpo_ctx* h) {
+  const int n = h->n, d = h->d, chi = h->chi, dd = d * d;
+  cudaStream_t st = h->stream;
+  int rc;
+  if ((rc = grow(h, h->env_l, (size_t)(n + 1) * chi * sizeof(cplx)))) return rc;
+  if ((rc = grow(h, h->env_r, (size_t)(n + 1) * chi * sizeof(cplx)))) return rc;
+  std::vector<int> dims(n + 1);
+  for (int b = 0; b <= n; ++b) {
+    int s = 0;
+    for (int q = 0; q < dd; ++q) s += h->cnt[(size_t)b * dd + q];
+    dims[b] = s;
+  }
+  if ((rc = grow(h, h->dims, (size_t)(n + 1) * sizeof(int)))) return rc;
+  if ((rc = grow_host(h, h->stage2, std::max<size_t>(h->stage2.bytes, (n + 1) * sizeof(int))))) return rc;
+  std::memcpy(h->stage2.p, dims.data(), (n + 1) * sizeof(int));
+  CK(h, cudaMemcpyAsync(h->dims.p, h->stage2.p, (n + 1) * sizeof(int), cudaMemcpyHostToDevice, st));
+  cplx* R = reinterpret_cast<cplx*>(h->env_r.p);
+  cplx* Lv = reinterpret_cast<cplx*>(h->env_l.p);
+  const int64_t chi2 = (int64_t)chi * chi;
+  CKL(h, launch_env_init(d, chi, h->charge + (size_t)n * chi * 2, h->lam + (size_t)n * chi,
+                         R + (size_t)n * chi, st));
+  for (int b = n - 1; b >= 0; --b)
+    CKL(h, launch_env_right_step(d, chi, h->gamma + (size_t)b * chi2, h->charge + (size_t)b * chi * 2,
+                                 h->lam + (size_t)b * chi, R + (size_t)(b + 1) * chi,
+                                 R + (size_t)b * chi, dims[b], dims[b + 1], st));
+  CKL(h, launch_env_init(d, chi, h->charge, h->lam, Lv, st));
+  for (int b = 0; b < n; ++b)
+    CKL(h, launch_env_left_step(d, chi, h->gamma + (size_t)b * chi2,
+                                h->charge + (size_t)(b + 1) * chi * 2, h->lam + (size_t)(b + 1) * chi,
+                                Lv + (size_t)b * chi, Lv + (size_t)(b + 1) * chi, dims[b], dims[b + 1],
+                                st));
+  return BSMPO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bsmpo_version(void) { return "bsmpo 0.1 (sm_100a, FP64 plain path)"; }
+
+const char* bsmpo_last_error(const bsmpo_ctx* h) {
+  if (h) return h->err.c_str();
+  return g_last_error.c_str();
+}
+
+int bsmpo_unitary(int d, const double* M, void* u_out, void* stream) {
+  if (d < 1 || d > BSMPO_MAX_D || !M || !u_out) return fail(nullptr, BSMPO_EINVAL, "bad argument");
+  M8 m;
+  for (int i = 0; i < 8; ++i) m.v[i] = M[i];
+  cudaError_t e = launch_fock_tensor_single(d, m, u_out, nullptr, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(nullptr, BSMPO_ECUDA, cudaGetErrorString(e));
+  return BSMPO_OK;
+}
+
+int bsmpo_unitary_tr(int d, double t_re, double t_im, double r_re, double r_im, double* u_re,
+                     double* u_im, void* stream) {
+  if (d < 1 || d > BSMPO_MAX_D || !u_re || !u_im) return fail(nullptr, BSMPO_EINVAL, "bad argument");
+  // M = [[t, -conj r], [r, conj t]]
+  M8 m;
+  m.v[0] = t_re; m.v[1] = t_im;
+  m.v[2] = -r_re; m.v[3] = r_im;
+  m.v[4] = r_re; m.v[5] = r_im;
+  m.v[6] = t_re; m.v[7] = -t_im;
+  cudaError_t e = launch_fock_tensor_single(d, m, u_re, u_im, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(nullptr, BSMPO_ECUDA, cudaGetErrorString(e));
+  return BSMPO_OK;
+}
+
+int bsmpo_contract_sector(int d, int cc0, int cc1, const void* u, const void* glc, const void* gcr,
+                          const int* cl, const int* cc, const int* cr, int len_l, int len_c,
+                          int len_r, void* c, void* stream) {
+  if (d < 1 || d > BSMPO_MAX_D || len_l < 0 || len_c < 0 || len_r < 0 || !u || !c)
+    return fail(nullptr, BSMPO_EINVAL, "bad argument");
+  if (cc0 < 0 || cc1 < 0 || cc0 >= d || cc1 >= d) return fail(nullptr, BSMPO_EINVAL, "bad centre charge");
+  cudaError_t e = launch_contract_sector(d, cc0, cc1, u, glc, gcr, cl, cc, cr, len_l, len_c, len_r, c,
+                                         (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(nullptr, BSMPO_ECUDA, cudaGetErrorString(e));
+  return BSMPO_OK;
+}
+
+int bsmpo_create(int n, int d, int chi, int flags, bsmpo_ctx** out) {
+  if (!out) return fail(nullptr, BSMPO_EINVAL, "null output handle");
+  *out = nullptr;
+  if (n < 2 || d < 1 || d > BSMPO_MAX_D || chi < 1 || chi > 8192 || flags != 0)
+    return fail(nullptr, BSMPO_EINVAL, "bad create arguments");
+  bsmpo_ctx* h = new bsmpo_ctx();
+  h->n = n; h->d = d; h->chi = chi;
+  cudaGetDevice(&h->device);
+  const size_t gbytes = (size_t)n * chi * chi * sizeof(cplx);
+  if (cudaMalloc(&h->gamma, gbytes) != cudaSuccess ||
+      cudaMalloc(&h->lam, (size_t)(n + 1) * chi * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->charge, (size_t)(n + 1) * chi * 2 * sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(h->gamma); cudaFree(h->lam); cudaFree(h->charge);
+    delete h;
+    return fail(nullptr, BSMPO_ENOMEM, "state allocation failed");
+  }
+  h->cnt.assign((size_t)(n + 1) * d * d, 0);
+  *out = h;
+  return BSMPO_OK;
+}
+
+int bsmpo_destroy(bsmpo_ctx* h) {
+  if (!h) return BSMPO_OK;
+  cudaStreamSynchronize(h->stream);
+  DevBuf* bufs[] = {&h->theta, &h->cbuf, &h->abuf, &h->wbuf, &h->vbuf, &h->sig, &h->keys,
+                    &h->perm, &h->tab, &h->tab2, &h->rot, &h->kept, &h->u3, &h->m4,
+                    &h->env_l, &h->env_r, &h->part, &h->outv, &h->dims};
+  for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
+  HostStage* hs[] = {&h->stage, &h->stage2, &h->hres};
+  for (HostStage* b : hs) if (b->p) cudaFreeHost(b->p);
+  cudaFree(h->gamma); cudaFree(h->lam); cudaFree(h->charge);
+  delete h;
+  return BSMPO_OK;
+}
+
+int bsmpo_set_stream(bsmpo_ctx* h, void* stream) {
+  if (!h) return fail(nullptr, BSMPO_EINVAL, "null handle");
+  h->stream = (cudaStream_t)stream;
+  return BSMPO_OK;
+}
+
+int bsmpo_set_cutoff(bsmpo_ctx* h, double cutoff) {
+  if (!h) return fail(nullptr, BSMPO_EINVAL, "null handle");
+  if (!(cutoff >= 0.0) || cutoff >= 1.0) return fail(h, BSMPO_EINVAL, "cutoff must be in [0, 1)");
+  h->cutoff = cutoff;
+  return BSMPO_OK;
+}
+
+int bsmpo_load_state(bsmpo_ctx* h, const void* gamma, const double* lambda, const int* charge) {
+  if (!h || !gamma || !lambda || !charge) return fail(h, BSMPO_EINVAL, "null argument");
+  const int n = h->n, d = h->d, chi = h->chi;
+  cudaStream_t st = h->stream;
+  CK(h, cudaMemcpyAsync(h->gamma, gamma, (size_t)n * chi * chi * sizeof(cplx),
+                        cudaMemcpyDeviceToDevice, st));
+  CK(h, cudaMemcpyAsync(h->lam + chi, lambda, (size_t)(n - 1) * chi * sizeof(double),
+                        cudaMemcpyDeviceToDevice, st));
+  CK(h, cudaMemcpyAsync(h->charge, charge, (size_t)(n + 1) * chi * 2 * sizeof(int),
+                        cudaMemcpyDeviceToDevice, st));
+  std::vector<int> hc((size_t)(n + 1) * chi * 2);
+  std::vector<double> hl((size_t)(n + 1) * chi, 0.0);
+  CK(h, cudaMemcpyAsync(hc.data(), charge, hc.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(h, cudaMemcpyAsync(hl.data() + chi, lambda, (size_t)(n - 1) * chi * sizeof(double),
+                        cudaMemcpyDeviceToHost, st));
+  CK(h, cudaStreamSynchronize(st));
+  // validate: sorted, occupied slots first, charges in range, Lambda > 0 on occupied slots
+  std::fill(h->cnt.begin(), h->cnt.end(), 0);
+  for (int b = 0; b <= n; ++b) {
+    bool empty_seen = false;
+    int p0 = -1, p1 = -1;
+    for (int i = 0; i < chi; ++i) {
+      const int c0 = hc[((size_t)b * chi + i) * 2], c1 = hc[((size_t)b * chi + i) * 2 + 1];
+      const bool occ = c0 < d;
+      if (!occ) {
+        if (c0 != d || c1 != d)
+          return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": empty slots must carry (d, d)");
+        empty_seen = true;
+        if (b > 0 && b < n && hl[(size_t)b * chi + i] != 0.0)
+          return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": Lambda on an empty slot");
+        continue;
+      }
+      if (empty_seen) return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": occupied slot after an empty one");
+      if (c0 < 0 || c1 < 0 || c1 >= d) return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": charge out of range");
+      if (c0 < p0 || (c0 == p0 && c1 < p1))
+        return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": charges not sorted");
+      if (b > 0 && b < n && !(hl[(size_t)b * chi + i] > 0.0))
+        return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": occupied slot with Lambda <= 0");
+      p0 = c0; p1 = c1;
+      h->cnt[(size_t)b * d * d + c0 * d + c1]++;
+    }
+  }
+  // edge Lambda: 1 on occupied slots of bonds 0 and n
+  for (int b : {0, n})
+    for (int i = 0; i < chi; ++i) hl[(size_t)b * chi + i] = hc[((size_t)b * chi + i) * 2] < d ? 1.0 : 0.0;
+  CK(h, cudaMemcpyAsync(h->lam, hl.data(), chi * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(h, cudaMemcpyAsync(h->lam + (size_t)n * chi, hl.data() + (size_t)n * chi, chi * sizeof(double),
+                        cudaMemcpyHostToDevice, st));
+  CK(h, cudaStreamSynchronize(st));
+  h->loaded = true;
+  return BSMPO_OK;
+}
+
+int bsmpo_store_state(bsmpo_ctx* h, void* gamma, double* lambda, int* charge) {
+  if (!h || !h->loaded) return fail(h, BSMPO_EINVAL, "no state loaded");
+  const int n = h->n, chi = h->chi;
+  cudaStream_t st = h->stream;
+  if (gamma) CK(h, cudaMemcpyAsync(gamma, h->gamma, (size_t)n * chi * chi * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
+  if (lambda) CK(h, cudaMemcpyAsync(lambda, h->lam + chi, (size_t)(n - 1) * chi * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  if (charge) CK(h, cudaMemcpyAsync(charge, h->charge, (size_t)(n + 1) * chi * 2 * sizeof(int), cudaMemcpyDeviceToDevice, st));
+  CK(h, cudaStreamSynchronize(st));
+  return BSMPO_OK;
+}
+
+int bsmpo_bs_update_tensor(bsmpo_ctx* h, int mode, const void* u) {
+  if (!u) return fail(h, BSMPO_EINVAL, "null tensor");
+  return bs_update_impl(h, mode, reinterpret_cast<const cplx*>(u));
+}
+
+int bsmpo_bs_update(bsmpo_ctx* h, int mode, const double* S) {
+  int rc = check_mode(h, mode);
+  if (rc) return rc;
+  if (!S) return fail(h, BSMPO_EINVAL, "null matrix");
+  const int d = h->d;
+  if ((rc = grow(h, h->u3, (size_t)d * d * d * sizeof(cplx)))) return rc;
+  CKL(h, launch_fock_tensor_single(d, transpose_to_m8(S), h->u3.p, nullptr, h->stream));
+  return bs_update_impl(h, mode, reinterpret_cast<const cplx*>(h->u3.p));
+}
+
+int bsmpo_run_mesh(bsmpo_ctx* h, int n_bs, const int* modes, const double* theta, const double* phi) {
+  if (!h || n_bs < 0 || (n_bs > 0 && (!modes || !theta || !phi))) return fail(h, BSMPO_EINVAL, "bad argument");
+  if (!h->loaded) return fail(h, BSMPO_EINVAL, "no state loaded");
+  if (n_bs == 0) return BSMPO_OK;
+  const int d = h->d, d3 = d * d * d;
+  int rc;
+  for (int i = 0; i < n_bs; ++i)
+    if (modes[i] < 0 || modes[i] > h->n - 2) return fail(h, BSMPO_EINVAL, "mode out of range");
+  if ((rc = grow(h, h->u3, (size_t)n_bs * d3 * sizeof(cplx)))) return rc;
+  if ((rc = grow(h, h->m4, (size_t)n_bs * 8 * sizeof(double)))) return rc;
+  std::vector<double> m4((size_t)n_bs * 8);
+  for (int i = 0; i < n_bs; ++i) {
+    // T(theta, phi) = [[e^{i phi} c, -s], [e^{i phi} s, c]]; tensor of M = T^T
+    const double c = std::cos(theta[i]), s = std::sin(theta[i]);
+    const double er = std::cos(phi[i]), ei = std::sin(phi[i]);
+    double S[8] = {er * c, ei * c, -s, 0.0, er * s, ei * s, c, 0.0};
+    M8 m = transpose_to_m8(S);
+    for (int j = 0; j < 8; ++j) m4[(size_t)i * 8 + j] = m.v[j];
+  }
+  if ((rc = grow_host(h, h->stage2, std::max(h->stage2.bytes, m4.size() * sizeof(double))))) return rc;
+  std::memcpy(h->stage2.p, m4.data(), m4.size() * sizeof(double));
+  CK(h, cudaMemcpyAsync(h->m4.p, h->stage2.p, m4.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CKL(h, launch_fock_tensor(d, n_bs, reinterpret_cast<const double*>(h->m4.p), h->u3.p, h->stream));
+  // the stage is reused by the updates: make sure the copy has been consumed
+  CK(h, cudaStreamSynchronize(h->stream));
+  for (int i = 0; i < n_bs; ++i) {
+    rc = bs_update_impl(h, modes[i], reinterpret_cast<const cplx*>(h->u3.p) + (size_t)i * d3);
+    if (rc) return rc;
+  }
+  return BSMPO_OK;
+}
+
+int bsmpo_apply_phases(bsmpo_ctx* h, const double* phases) {
+  if (!h || !phases) return fail(h, BSMPO_EINVAL, "bad argument");
+  if (!h->loaded) return fail(h, BSMPO_EINVAL, "no state loaded");
+  const int chi = h->chi;
+  for (int m = 0; m < h->n; ++m)
+    CKL(h, launch_phase(h->d, chi, phases[m], h->charge + (size_t)m * chi * 2,
+                        h->charge + (size_t)(m + 1) * chi * 2, h->gamma + (size_t)m * chi * chi,
+                        h->stream));
+  return BSMPO_OK;
+}
+
+int bsmpo_observables(bsmpo_ctx* h, double* trace, double* marginals) {
+  if (!h || !trace) return fail(h, BSMPO_EINVAL, "bad argument");
+  if (!h->loaded) return fail(h, BSMPO_EINVAL, "no state loaded");
+  const int n = h->n, d = h->d, chi = h->chi;
+  int rc;
+  if ((rc = env_all(h))) return rc;
+  const int chunk_rows = 32;
+  const int nchunk = ceil_div(chi, chunk_rows);
+  if ((rc = grow(h, h->part, (size_t)n * nchunk * d * sizeof(cplx)))) return rc;
+  if ((rc = grow(h, h->outv, ((size_t)n * d + 1) * sizeof(cplx)))) return rc;
+  cplx* out = reinterpret_cast<cplx*>(h->outv.p);
+  CKL(h, launch_sum_vector(h->env_r.p, chi, out + (size_t)n * d, h->stream));
+  if (marginals)
+    CKL(h, launch_marginals(n, d, chi, h->gamma, h->charge, h->env_l.p, h->env_r.p,
+                            reinterpret_cast<const int*>(h->dims.p), h->part.p, chunk_rows, out,
+                            h->stream));
+  if ((rc = grow_host(h, h->hres, std::max(h->hres.bytes, ((size_t)n * d + 1) * sizeof(cplx) + 8192)))) return rc;
+  cplx* ho = reinterpret_cast<cplx*>(static_cast<char*>(h->hres.p) + 4096);
+  CK(h, cudaMemcpyAsync(ho, out, ((size_t)n * d + 1) * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  trace[0] = ho[(size_t)n * d].x;
+  trace[1] = ho[(size_t)n * d].y;
+  if (marginals)
+    for (int i = 0; i < n * d; ++i) { marginals[2 * i] = ho[i].x; marginals[2 * i + 1] = ho[i].y; }
+  return BSMPO_OK;
+}
+
+int bsmpo_last_update_info(const bsmpo_ctx* hc, int* n_sectors, int* sector_cc, int* shape,
+                           int* sigma_len, double* sigma, int sigma_cap, int* kept,
+                           double* trunc_weight) {
+  bsmpo_ctx* h = const_cast<bsmpo_ctx*>(hc);
+  if (!h) return fail(nullptr, BSMPO_EINVAL, "null handle");
+  const int ns = h->last_ns;
+  if (n_sectors) *n_sectors = ns;
+  if (sector_cc) std::copy(h->last_cc.begin(), h->last_cc.end(), sector_cc);
+  if (shape) std::copy(h->last_shape.begin(), h->last_shape.end(), shape);
+  if (sigma_len) std::copy(h->last_k.begin(), h->last_k.end(), sigma_len);
+  if (kept) std::copy(h->last_kept.begin(), h->last_kept.end(), kept);
+  if (trunc_weight) *trunc_weight = h->last_trunc;
+  if (sigma) {
+    int64_t tot = 0;
+    for (int k : h->last_k) tot += k;
+    if (tot > sigma_cap) return fail(h, BSMPO_ECAPACITY, "sigma buffer too small");
+    CK(h, cudaMemcpyAsync(sigma, h->sig.p, tot * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+  }
+  return BSMPO_OK;
+}
+
+int bsmpo_last_update_work(const bsmpo_ctx* h, double* gemm_flops, double* svd_flops,
+                           double* min_bytes) {
+  if (!h) return fail(nullptr, BSMPO_EINVAL, "null handle");
+  if (gemm_flops) *gemm_flops = h->last_gemm;
+  if (svd_flops) *svd_flops = h->last_svd;
+  if (min_bytes) *min_bytes = h->last_bytes;
+  return BSMPO_OK;
+}
+
+int bsmpo_bond_dims(const bsmpo_ctx* h, int* dims) {
+  if (!h || !dims) return fail(nullptr, BSMPO_EINVAL, "bad argument");
+  const int dd = h->d * h->d;
+  for (int b = 0; b <= h->n; ++b) {
+    int s = 0;
+    for (int q = 0; q < dd; ++q) s += h->cnt[(size_t)b * dd + q];
+    dims[b] = s;
+  }
+  return BSMPO_OK;
+}
+
+int64_t bsmpo_kernel_launches(const bsmpo_ctx* h) { return h ? h->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,156 @@
+// Internal launch interface of libbsmpo's kernels (host side, C++).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+// Largest local cutoff d supported (charge tables are d x d).
+#define BSMPO_MAX_D 8
+#define BSMPO_MAX_Q (BSMPO_MAX_D * BSMPO_MAX_D)
+
+// ---------------------------------------------------------------- fock.cu
+cudaError_t launch_fock_tensor(int d, int n_gates, const double* m4_dev, void* u_dev,
+                               cudaStream_t s);
+// One gate with M passed by value; writes interleaved complex (u_im == nullptr) or
+// split real / imaginary double arrays.
+struct M8 { double v[8]; };
+cudaError_t launch_fock_tensor_single(int d, M8 m, void* u_re_or_cplx, double* u_im,
+                                      cudaStream_t s);
+
+// ---------------------------------------------------------------- zgemm.cu
+// One group of a grouped complex128 GEMM:  C = rs[m] cs[n] sum_k op(A)(m,k) ks[k] op(B)(k,n)
+// op 0: as stored (row-major A[m][k], B[k][n]); op 1: conjugate transpose (A stored
+// [k][m], B stored [n][k]).  Offsets are in complex elements (scales in doubles) from
+// the launch's base pointers; a negative scale offset means "none".
+struct GemmGroup {
+  int M, N, K;
+  int lda, ldb, ldc;
+  int opA, opB;
+  int beta;          // 0: C = result, 1: C += result
+  int tiles_n;       // ceil(N / tile N)
+  int tile_start;    // first flat tile index of this group
+  int pad_;
+  int64_t a_off, b_off, c_off;
+  int64_t ks_off, rs_off, cs_off;
+};
+
+cudaError_t launch_zgemm_grouped(const void* a, const void* b, void* c, const double* scale,
+                                 const GemmGroup* groups_dev, int n_groups, int total_tiles,
+                                 cudaStream_t s);
+int zgemm_tile_m();
+int zgemm_tile_n();
+
+// ---------------------------------------------------------------- plan descriptors
+// Theta group (q, a0, b0): Theta_q[rows of left group a0 with a1 >= q1]
+//                                 [cols of right group b0 with b1 <= q1]
+//                         = Glc[rows][centre block q] @ Gcr[centre block q][cols]
+struct ThetaDesc {
+  int q0, q1, a0, b0;
+  int row0, nrow, col0, ncol, k0, nk;
+  int64_t off;            // storage [nrow][ncol] in the Theta workspace
+};
+
+struct SectorDesc {
+  int cc0, cc1;
+  int m, n;            // |L_s|, |R_s|
+  int k;               // columns of the Jacobi matrix: n when !left, m when left
+  int left;            // 1: Jacobi on [T^H; I_m] (m < n), 0: on T (m >= n)
+  int rows_g;          // rows entering the pair Gram (m or n)
+  int rows_tot;        // stored rows of the Jacobi matrix (m or n + m)
+  int kept;            // filled after selection
+  int slot0;           // first slot of this sector on the new bond
+  int64_t c_off;       // C[m][n] row-major (complex)
+  int64_t a_off;       // Jacobi matrix, row-major [rows_tot][k] (complex)
+  int64_t s_off;       // singular values / keys / permutation (k entries)
+  int64_t w_off;       // W = V^H C, [kept][n] row-major (complex)
+  int64_t v_off;       // conj(V) rows, [kept][m] row-major (complex)
+  int row_start[BSMPO_MAX_D];   // row of L_s where left group a0 (a1 >= cc1 part) starts
+  int col_start[BSMPO_MAX_D];   // column of R_s where right group b0 (b1 <= cc1 part) starts
+};
+
+// One (left block a, right block b), a >= b, of the gate mix, cut in tiles of 256 elements.
+struct MixPair {
+  int a0, a1, b0, b1;
+  int row0, nrow;      // left-bond rows of block a
+  int col0, ncol;      // right-bond columns of block b
+  int tile_start;      // first flat CTA index of this pair
+  int pad_;
+};
+
+// Per-update tables shared by several kernels (device copy, one per update).
+struct UpdateTables {
+  int d, chi, mode;
+  int n_sectors, n_theta, n_pairs;
+  int offL[BSMPO_MAX_Q + 1], offC[BSMPO_MAX_Q + 1], offR[BSMPO_MAX_Q + 1];
+  int sidx[BSMPO_MAX_Q];                          // sector index of centre charge, or -1
+  int pair_of[BSMPO_MAX_Q];                       // sector index of the (cc1, cc0) sector, or -1
+};
+
+// ---------------------------------------------------------------- sector.cu
+// Theta -> C (every sector, row-major) and the Jacobi matrix (T or [T^H; I]).
+cudaError_t launch_mix_d(int d, const UpdateTables* tab_dev, const int* tidx_dev,
+                         const ThetaDesc* td_dev, const SectorDesc* sd_dev,
+                         const MixPair* pairs_dev, int n_pairs, int total_tiles, const void* u3,
+                         const void* theta, const double* lam_r, void* cbuf, void* abuf,
+                         cudaStream_t s);
+// Identity rows of [T^H; I_m] for the `left` sectors.
+cudaError_t launch_identity_rows(const SectorDesc* sd_dev, int n_sectors, int max_elems,
+                                 void* abuf, cudaStream_t s);
+// Deterministic top-chi with ket/bra pair symmetrisation; writes kept counts into
+// sd_dev[s].kept and kept_out[s], slot starts, and the truncation weight.
+cudaError_t launch_select(const UpdateTables* tab_dev, SectorDesc* sd_dev, int n_sectors,
+                          const double* sig, double* keys, double cutoff, int chi,
+                          int* kept_out, double* trunc_out, cudaStream_t s);
+// conj(V) rows for the kept vectors of every sector.
+cudaError_t launch_extract_v(const SectorDesc* sd_dev, int n_sectors, int max_elems,
+                             const void* abuf, const double* sig, const int* perm, void* vbuf,
+                             cudaStream_t s);
+// New Gamma_L (= Gamma[mode]), Gamma_R (= Gamma[mode+1]), Lambda and charges of bond mode+1.
+cudaError_t launch_scatter(const UpdateTables* tab_dev, const SectorDesc* sd_dev, int n_sectors,
+                           int total_kept, int chi, const int* charge_l, const int* charge_r,
+                           const void* vbuf, const void* wbuf, const double* sig,
+                           void* gamma_l, void* gamma_r, double* lam_c, int* charge_c,
+                           cudaStream_t s);
+// exp(i phi (n_ket - n_bra)) on every element of one site tensor.
+cudaError_t launch_phase(int d, int chi, double phi, const int* charge_l, const int* charge_r,
+                         void* gamma, cudaStream_t s);
+
+// ---------------------------------------------------------------- jacobi.cu
+// One round of the blocked one-sided Jacobi SVD for every active sector.
+struct JacobiWork {
+  int sector;       // index into the SectorDesc array
+  int nblk;         // column blocks
+  int npairs;       // CTAs per round (block pairs)
+  int rounds;       // rounds per sweep
+  int cta_start;    // first flat CTA index of this sector
+  int pad_;
+};
+int jacobi_block_cols();
+cudaError_t launch_jacobi_round(const SectorDesc* sd_dev, const JacobiWork* work_dev, int n_work,
+                                int total_ctas, int t, void* abuf, int* rot_count, double tol,
+                                int max_sweeps, cudaStream_t s);
+// Column norms, descending sort (ties by column index): sig[s_off..], perm[s_off..].
+cudaError_t launch_jacobi_finish(const SectorDesc* sd_dev, int n_sectors, int max_k,
+                                 const void* abuf, double* sig, int* perm, cudaStream_t s);
+
+// ---------------------------------------------------------------- contract.cu
+// Standalone sector contraction with per-element charges (the update_MPO drop-in).
+cudaError_t launch_contract_sector(int d, int cc0, int cc1, const void* u, const void* glc,
+                                   const void* gcr, const int* cl, const int* cc, const int* cr,
+                                   int len_l, int len_c, int len_r, void* c, cudaStream_t s);
+
+// ---------------------------------------------------------------- observables.cu
+// env_r[b] (b = n..0) and env_l[b] (b = 0..n), complex, masked to ket == bra charges.
+cudaError_t launch_env_right_step(int d, int chi, const void* gamma_b, const int* charge_b,
+                                  const double* lam_b, const void* r_next, void* r_out,
+                                  int rows, int cols, cudaStream_t s);
+cudaError_t launch_env_left_step(int d, int chi, const void* gamma_b, const int* charge_next,
+                                 const double* lam_next, const void* l_cur, void* l_out,
+                                 int rows, int cols, cudaStream_t s);
+cudaError_t launch_env_init(int d, int chi, const int* charge_b, const double* lam_b, void* v,
+                            cudaStream_t s);
+// partial marginal bins: part[site][chunk][d] complex, then reduced into out[site][d].
+cudaError_t launch_marginals(int n, int d, int chi, const void* gamma, const int* charge,
+                             const void* env_l, const void* env_r, const int* dims,
+                             void* part, int chunk_rows, void* out, cudaStream_t s);
+cudaError_t launch_sum_vector(const void* v, int len, void* out, cudaStream_t s);

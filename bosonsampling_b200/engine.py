@@ -1,0 +1,254 @@
+"""Device-resident MPO simulator over libbsmpo (the product path).
+
+``MPOSimulator`` owns one libbsmpo handle: the MPO lives in HBM for the whole run,
+every beam-splitter update runs as CUDA kernels, and only the per-update kept counts
+(and observables, when asked for) come back to the host.  PyTorch provides device
+memory and the current stream; it does no arithmetic on the update path.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _capi
+
+
+def product_state(n_modes, rho_sites, d, chi, total_photons=None):
+    """Product-state MPO with U(1) charges (the reference's ``Initialize`` filling,
+    ``src/MPO.py:56-109``, for arbitrary input modes).
+
+    ``rho_sites[i]`` is mode i's d x d density matrix.  Bond charges are the (ket, bra)
+    photon numbers to the right of the bond, capped at d-1; bond 0 lists every diagonal
+    total (c, c), c < d (or only the post-selected total).  Returns host arrays
+    ``Gamma[n, chi, chi]`` complex128, ``Lambda[n-1, chi]`` float64 (1 on occupied
+    slots) and ``charge[n+1, chi, 2]`` int32 (sentinel d on empty slots).
+    """
+    bonds = [None] * (n_modes + 1)
+    bonds[n_modes] = [(0, 0)]
+    for b in range(n_modes - 1, -1, -1):
+        rho = rho_sites[b]
+        s = set()
+        for (c0, c1) in bonds[b + 1]:
+            for o0 in range(d):
+                for o1 in range(d):
+                    if rho[o0, o1] != 0 and c0 + o0 <= d - 1 and c1 + o1 <= d - 1:
+                        s.add((c0 + o0, c1 + o1))
+        if b == 0:
+            s = {(c, c) for c in range(d)} if total_photons is None else {(total_photons, total_photons)}
+        bonds[b] = sorted(s)
+        if len(bonds[b]) > chi:
+            raise ValueError("chi=%d is smaller than the product-state bond dimension %d" % (chi, len(bonds[b])))
+    gamma = np.zeros((n_modes, chi, chi), dtype=np.complex128)
+    lam = np.zeros((n_modes - 1, chi), dtype=np.float64)
+    charge = np.full((n_modes + 1, chi, 2), d, dtype=np.int32)
+    for b in range(n_modes + 1):
+        for i, c in enumerate(bonds[b]):
+            charge[b, i] = c
+        if 0 < b < n_modes:
+            lam[b - 1, :len(bonds[b])] = 1.0
+    for site in range(n_modes):
+        rho = rho_sites[site]
+        for i, (a0, a1) in enumerate(bonds[site]):
+            for j, (b0, b1) in enumerate(bonds[site + 1]):
+                o0, o1 = a0 - b0, a1 - b1
+                if 0 <= o0 < d and 0 <= o1 < d:
+                    gamma[site, i, j] = rho[o0, o1]
+    return gamma, lam, charge
+
+
+def lossy_single_photon_rhos(n_modes, photon_modes, eta, d):
+    """(1-eta)|0><0| + eta|1><1| on ``photon_modes``, vacuum elsewhere."""
+    pm = set(int(m) for m in photon_modes)
+    out = []
+    for i in range(n_modes):
+        rho = np.zeros((d, d), dtype=np.complex128)
+        if i in pm:
+            rho[0, 0] = 1.0 - eta
+            if d > 1:
+                rho[1, 1] = eta
+        else:
+            rho[0, 0] = 1.0
+        out.append(rho)
+    return out
+
+
+def clements_t(theta, phi):
+    """2x2 block of T(theta, phi) = [[e^{i phi} cos, -sin], [e^{i phi} sin, cos]]."""
+    c, s = np.cos(theta), np.sin(theta)
+    e = np.exp(1j * phi)
+    return np.array([[e * c, -s], [e * s, c]], dtype=np.complex128)
+
+
+def _m8(S):
+    S = np.asarray(S, dtype=np.complex128)
+    return np.array([S[0, 0].real, S[0, 0].imag, S[0, 1].real, S[0, 1].imag,
+                     S[1, 0].real, S[1, 0].imag, S[1, 1].real, S[1, 1].imag], dtype=np.float64)
+
+
+class MPOSimulator:
+    """One n-mode, cutoff-d, bond-dimension-chi MPO resident on the current CUDA device."""
+
+    def __init__(self, n, d, chi, cutoff=0.0):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("MPOSimulator needs a CUDA device (no CPU path exists)")
+        self.torch = torch
+        self.n, self.d, self.chi = int(n), int(d), int(chi)
+        self.L = _capi.lib()
+        h = ctypes.c_void_p()
+        _capi.check(self.L.bsmpo_create(self.n, self.d, self.chi, 0, ctypes.byref(h)))
+        self.h = h
+        self.set_stream(torch.cuda.current_stream())
+        self.set_cutoff(cutoff)
+
+    # -------------------------------------------------------------- plumbing
+    def _chk(self, rc):
+        _capi.check(rc, self.h)
+
+    def set_stream(self, stream):
+        self._stream = stream
+        self._chk(self.L.bsmpo_set_stream(self.h, ctypes.c_void_p(stream.cuda_stream)))
+
+    def set_cutoff(self, cutoff):
+        self._chk(self.L.bsmpo_set_cutoff(self.h, float(cutoff)))
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.bsmpo_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -------------------------------------------------------------- state
+    def load(self, gamma, lam, charge):
+        """Load device tensors (complex128 [n,chi,chi], float64 [n-1,chi], int32 [n+1,chi,2])."""
+        t = self.torch
+        g = gamma.to(dtype=t.complex128).contiguous()
+        l = lam.to(dtype=t.float64).contiguous()
+        c = charge.to(dtype=t.int32).contiguous()
+        assert g.is_cuda and l.is_cuda and c.is_cuda
+        assert tuple(g.shape) == (self.n, self.chi, self.chi)
+        assert tuple(l.shape) == (self.n - 1, self.chi)
+        assert tuple(c.shape) == (self.n + 1, self.chi, 2)
+        self._chk(self.L.bsmpo_load_state(self.h, ctypes.c_void_p(g.data_ptr()),
+                                          ctypes.c_void_p(l.data_ptr()),
+                                          ctypes.c_void_p(c.data_ptr())))
+
+    def load_host(self, gamma, lam, charge):
+        t = self.torch
+        dev = t.device("cuda", t.cuda.current_device())
+        self.load(t.from_numpy(np.ascontiguousarray(gamma)).to(dev),
+                  t.from_numpy(np.ascontiguousarray(lam)).to(dev),
+                  t.from_numpy(np.ascontiguousarray(charge)).to(dev))
+
+    def store(self):
+        """Device tensors (Gamma, Lambda, charge) copied out of the handle."""
+        t = self.torch
+        dev = t.device("cuda", t.cuda.current_device())
+        g = t.empty((self.n, self.chi, self.chi), dtype=t.complex128, device=dev)
+        l = t.empty((self.n - 1, self.chi), dtype=t.float64, device=dev)
+        c = t.empty((self.n + 1, self.chi, 2), dtype=t.int32, device=dev)
+        self._chk(self.L.bsmpo_store_state(self.h, ctypes.c_void_p(g.data_ptr()),
+                                           ctypes.c_void_p(l.data_ptr()),
+                                           ctypes.c_void_p(c.data_ptr())))
+        return g, l, c
+
+    def init_product(self, rho_sites, total_photons=None, canonicalize=True):
+        g, l, c = product_state(self.n, rho_sites, self.d, self.chi, total_photons)
+        self.load_host(g, l, c)
+        if canonicalize:
+            self.canonicalize()
+
+    def init_single_photons(self, photon_modes, eta, total_photons=None):
+        """Lossy single photons (transmissivity eta) in ``photon_modes``, canonicalised."""
+        self.init_product(lossy_single_photon_rhos(self.n, photon_modes, eta, self.d), total_photons)
+
+    def canonicalize(self):
+        """Right-to-left sweep of identity-gate updates (``src/MPO.py:137-155``)."""
+        eye = _m8(np.eye(2))
+        for mode in range(self.n - 2, -1, -1):
+            self._chk(self.L.bsmpo_bs_update(self.h, mode, _capi.dptr(eye)))
+
+    # -------------------------------------------------------------- updates
+    def bs_update(self, mode, S):
+        """Apply the 2x2 single-particle unitary ``S`` to modes (mode, mode+1)."""
+        m = _m8(S)
+        self._chk(self.L.bsmpo_bs_update(self.h, int(mode), _capi.dptr(m)))
+
+    def bs_update_tensor(self, mode, U3):
+        """Apply a gate given as a device tensor U[new_a, new_b, old_a] (complex128 d^3)."""
+        u = U3.to(dtype=self.torch.complex128).contiguous()
+        assert u.is_cuda and u.numel() == self.d ** 3
+        self._chk(self.L.bsmpo_bs_update_tensor(self.h, int(mode), ctypes.c_void_p(u.data_ptr())))
+
+    def run_mesh(self, modes, theta, phi):
+        modes = np.ascontiguousarray(modes, dtype=np.int32)
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        self._chk(self.L.bsmpo_run_mesh(self.h, len(modes), _capi.iptr(modes), _capi.dptr(theta),
+                                        _capi.dptr(phi)))
+
+    def apply_phases(self, phases):
+        ph = np.ascontiguousarray(phases, dtype=np.float64)
+        assert ph.shape == (self.n,)
+        self._chk(self.L.bsmpo_apply_phases(self.h, _capi.dptr(ph)))
+
+    # -------------------------------------------------------------- results
+    def observables(self, marginals=True):
+        """(trace complex, P[n, d] complex or None) in FP64."""
+        tr = np.zeros(2)
+        P = np.zeros((self.n, self.d, 2)) if marginals else None
+        self._chk(self.L.bsmpo_observables(self.h, _capi.dptr(tr),
+                                           _capi.dptr(P) if marginals else None))
+        Pc = (P[..., 0] + 1j * P[..., 1]) if marginals else None
+        return complex(tr[0], tr[1]), Pc
+
+    def trace(self):
+        return self.observables(marginals=False)[0]
+
+    def last_update_info(self):
+        ns = ctypes.c_int()
+        self._chk(self.L.bsmpo_last_update_info(self.h, ctypes.byref(ns), None, None, None, None, 0,
+                                                None, None))
+        n = ns.value
+        cc = np.zeros((max(n, 1), 2), dtype=np.int32)
+        shape = np.zeros((max(n, 1), 2), dtype=np.int32)
+        slen = np.zeros(max(n, 1), dtype=np.int32)
+        kept = np.zeros(max(n, 1), dtype=np.int32)
+        tw = np.zeros(1)
+        self._chk(self.L.bsmpo_last_update_info(self.h, ctypes.byref(ns), _capi.iptr(cc),
+                                                _capi.iptr(shape), _capi.iptr(slen), None, 0,
+                                                _capi.iptr(kept), _capi.dptr(tw)))
+        sig = np.zeros(max(int(slen[:n].sum()), 1))
+        self._chk(self.L.bsmpo_last_update_info(self.h, ctypes.byref(ns), None, None, None,
+                                                _capi.dptr(sig), len(sig), None, None))
+        offs = np.concatenate([[0], np.cumsum(slen[:n])])
+        return {
+            "sectors": [tuple(int(x) for x in cc[i]) for i in range(n)],
+            "shape": [tuple(int(x) for x in shape[i]) for i in range(n)],
+            "sigma": [sig[offs[i]:offs[i + 1]].copy() for i in range(n)],
+            "kept": [int(k) for k in kept[:n]],
+            "trunc_weight": float(tw[0]),
+        }
+
+    def last_update_work(self):
+        g, s, b = np.zeros(1), np.zeros(1), np.zeros(1)
+        self._chk(self.L.bsmpo_last_update_work(self.h, _capi.dptr(g), _capi.dptr(s), _capi.dptr(b)))
+        return {"gemm_flops": float(g[0]), "svd_flops": float(s[0]), "min_bytes": float(b[0])}
+
+    def bond_dims(self):
+        out = np.zeros(self.n + 1, dtype=np.int32)
+        self._chk(self.L.bsmpo_bond_dims(self.h, _capi.iptr(out)))
+        return [int(x) for x in out]
+
+    def kernel_launches(self):
+        return int(self.L.bsmpo_kernel_launches(self.h))

@@ -1,0 +1,146 @@
+/*
+ * bsmpo.h -- C ABI of libbsmpo.so, the B200 (sm_100a) beam-splitter MPO update.
+ *
+ * One BS update of a U(1)-symmetric density-matrix MPO = Fock beam-splitter tensor
+ * -> per-charge-block two-site contraction -> per-sector SVD -> top-chi truncation
+ * -> scatter into the two site tensors.  Everything runs on the device; the library
+ * owns the MPO state and its workspaces.
+ *
+ * Conventions
+ *   - Every function returns 0 on success and a negative BSMPO_E* code on failure;
+ *     bsmpo_last_error() gives a message.  No C++ exception crosses the ABI.
+ *   - Pointers documented "device" are CUDA device pointers; "host" pointers are
+ *     plain host memory.  `stream` arguments are cudaStream_t (NULL = legacy default).
+ *   - complex128 is interleaved (re, im) doubles.
+ *   - State layout (the reference's, src/MPO.py:114-132 and
+ *     src/beam_splitter_parallel/Full.py:56-63, in double precision):
+ *       gamma  [n][chi][chi] complex128   Gamma[site][left bond][right bond]
+ *       lambda [n-1][chi]    double       Lambda on bond i+1 (between sites i, i+1)
+ *       charge [n+1][chi][2] int32        (ket, bra) photons right of the bond,
+ *                                         sorted lexicographically, empty = (d, d)
+ *   - One handle is used from one host thread at a time.
+ */
+#ifndef BSMPO_H
+#define BSMPO_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BSMPO_OK 0
+#define BSMPO_EINVAL -1      /* bad argument / inconsistent state */
+#define BSMPO_ECUDA -2       /* CUDA runtime error */
+#define BSMPO_ENOMEM -3      /* device allocation failed */
+#define BSMPO_ECAPACITY -4   /* a workspace bound was exceeded */
+#define BSMPO_ECONVERGE -5   /* the per-sector SVD did not converge */
+
+typedef struct bsmpo_ctx bsmpo_ctx;
+
+/* Library version string. */
+const char* bsmpo_version(void);
+
+/* Message of the last error on `h` (or of the last handle-less call when h == NULL). */
+const char* bsmpo_last_error(const bsmpo_ctx* h);
+
+/* Two-mode Fock beam-splitter tensor.  Replaces cuda_kernels.Rand_U / u_kernel
+ * (src/cuda_kernels.py:18-50, src/u_kernel.cu:37-71) and the CPU Rand_BS_MPS
+ * (src/MPO.py:6-18).  M is the 2x2 single-particle matrix of the reference's
+ * convention, a+ -> M00 a+ + M10 b+, b+ -> M01 a+ + M11 b+ (for the reference's
+ * (t, r): M = [[t, -conj r], [r, conj t]]), given as 8 host doubles
+ * (re, im of M00, M01, M10, M11).  Writes U[n][m][l] = <l, n+m-l| M |n, m> for
+ * 0 <= n, m, l < d (zero where n+m-l is outside [0, d)) as complex128 to the device
+ * buffer u_out (d^3 entries).  Integer powers in FP64: exact at r = 0 and t = 0. */
+int bsmpo_unitary(int d, const double* M, void* u_out, void* stream);
+
+/* Same, for the reference's (t, r) pair, writing split real / imaginary parts
+ * (the layout of cuda_kernels.Rand_U): u_re, u_im are device double[d^3]. */
+int bsmpo_unitary_tr(int d, double t_re, double t_im, double r_re, double r_im,
+                     double* u_re, double* u_im, void* stream);
+
+/* One centre-charge sector of the two-site contraction.  Replaces
+ * cuda_kernels.update_MPO / update_MPO_kernel.cu:kernel (src/cuda_kernels.py:101-127,
+ * src/update_MPO_kernel.cu:193-733), without the reference's x8 alignment padding:
+ *   C[l][r] = sum_c Glc[l][c] Gcr[c][r] U(cl0-cc0, cc0-cr0, cl0-q0(c))
+ *                                       conj U(cl1-cc1, cc1-cr1, cl1-q1(c))
+ * over c with cl >= q(c) >= cr componentwise (else the term is 0).
+ *   u    device complex128 [d][d][d] (bsmpo_unitary output, U[new_a][new_b][old_a])
+ *   glc  device complex128 [len_l][len_c] row-major; gcr [len_c][len_r]
+ *   cl   device int32 [len_l][2]; cc [len_c][2] (sorted); cr [len_r][2]
+ *   c    device complex128 [len_l][len_r] output (overwritten). */
+int bsmpo_contract_sector(int d, int cc0, int cc1, const void* u,
+                          const void* glc, const void* gcr,
+                          const int* cl, const int* cc, const int* cr,
+                          int len_l, int len_c, int len_r, void* c, void* stream);
+
+/* Create a handle for an n-mode chain with local cutoff d and bond dimension chi.
+ * Allocates the device state (n chi^2 complex128) and workspaces on the current
+ * device.  flags: reserved, pass 0. */
+int bsmpo_create(int n, int d, int chi, int flags, bsmpo_ctx** out);
+int bsmpo_destroy(bsmpo_ctx* h);
+
+/* Stream used by all following calls on h (default: the legacy default stream). */
+int bsmpo_set_stream(bsmpo_ctx* h, void* stream);
+
+/* Relative singular-value cutoff: a singular value s is kept only if
+ * s > cutoff * (largest singular value of that update).  0 (the default) keeps every
+ * s > 0, the reference's rule (src/MPO.py:272-279 with the Lambda > 0 masks). */
+int bsmpo_set_cutoff(bsmpo_ctx* h, double cutoff);
+
+/* Copy a state into / out of the handle.  Device pointers in the layout above.
+ * load validates it (sorted charges, sentinel d for empty slots, Lambda > 0 on
+ * occupied internal slots). */
+int bsmpo_load_state(bsmpo_ctx* h, const void* gamma, const double* lambda, const int* charge);
+int bsmpo_store_state(bsmpo_ctx* h, void* gamma, double* lambda, int* charge);
+
+/* Apply a beam splitter to modes (mode, mode+1): the per-BS unit of work of
+ * RankWorker.RankProcess (src/beam_splitter_parallel/Rank.py:32-206) and
+ * InitializationMPO.Update (src/MPO.py:158-303), fully on the device.
+ * S: host double[8], the 2x2 single-particle unitary acting on the state
+ * (a photon entering mode j leaves mode i with amplitude S[i][j]). */
+int bsmpo_bs_update(bsmpo_ctx* h, int mode, const double* S);
+
+/* Same with an explicit device tensor U[new_a][new_b][old_a] (complex128 d^3), e.g.
+ * the reference's Rand_BS_MPS tensor or bsmpo_unitary output. */
+int bsmpo_bs_update_tensor(bsmpo_ctx* h, int mode, const void* u);
+
+/* Run a whole mesh (the walk of src/beam_splitter_parallel/Full.py:149-202):
+ * n_bs beam splitters T(theta, phi) = [[e^{i phi} cos, -sin], [e^{i phi} sin, cos]]
+ * on (modes[i], modes[i]+1), in the given order.  Host arrays. */
+int bsmpo_run_mesh(bsmpo_ctx* h, int n_bs, const int* modes, const double* theta,
+                   const double* phi);
+
+/* Output phase screen exp(i phase_m n_m) on every mode (host double[n]). */
+int bsmpo_apply_phases(bsmpo_ctx* h, const double* phases);
+
+/* Trace (summary.Probability, src/summary.py:11-26) and single-mode photon-number
+ * marginals P[i][k] = Prob(k photons in mode i), un-normalised, in FP64.
+ * Host outputs: trace[2] (re, im), marginals[n][d][2] (re, im); marginals may be NULL. */
+int bsmpo_observables(bsmpo_ctx* h, double* trace, double* marginals);
+
+/* Diagnostics of the last update (host buffers, capacities in entries):
+ *   n_sectors; per sector (in loop order) its centre charge sector_cc[s][2],
+ *   |L_s|, |R_s| in shape[s][2], the number of singular values sigma_len[s]
+ *   (descending, packed in sigma), the kept count kept[s]; and the truncation
+ *   weight (sum of discarded sigma^2).  Any output pointer may be NULL. */
+int bsmpo_last_update_info(const bsmpo_ctx* h, int* n_sectors, int* sector_cc, int* shape,
+                           int* sigma_len, double* sigma, int sigma_cap, int* kept,
+                           double* trunc_weight);
+
+/* Work counters of the last update (host): algorithmic flops of the contraction
+ * GEMMs and of the SVD step, and the bytes the update had to move at minimum. */
+int bsmpo_last_update_work(const bsmpo_ctx* h, double* gemm_flops, double* svd_flops,
+                           double* min_bytes);
+
+/* Bond dimensions (occupied slots) of every bond, host int[n+1]. */
+int bsmpo_bond_dims(const bsmpo_ctx* h, int* dims);
+
+/* Number of kernels this handle has launched since creation. */
+int64_t bsmpo_kernel_launches(const bsmpo_ctx* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BSMPO_H */
