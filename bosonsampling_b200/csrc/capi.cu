@@ -11,7 +11,9 @@
 //   blocked one-sided Jacobi rounds -> column norms + sort -> top-chi selection ->
 //   [sync: kept counts] -> V extraction -> W = V^H C grouped GEMM -> scatter.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -55,13 +57,23 @@ struct bsmpo_ctx {
   std::vector<int> cnt;
   // workspaces
   DevBuf theta, cbuf, abuf, wbuf, vbuf, sig, keys, perm, tab, tab2, rot, kept, u3, m4, env_l,
-      env_r, part, outv, dims;
+      env_r, part, outv, dims, nf2;
   HostStage stage, stage2, hres;
   // last update diagnostics (host)
   std::vector<int> last_cc, last_shape, last_kept, last_k;
   std::vector<int64_t> last_soff;
   double last_trunc = 0.0, last_gemm = 0.0, last_svd = 0.0, last_bytes = 0.0;
   int last_sweeps = 0;
+  // opt-in stage timing (BSMPO_PROFILE=1): synchronises after every stage
+  bool profile = false;
+  double stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int64_t jacobi_rounds = 0, updates = 0;
+  // Jacobi-phase timing with CUDA events (no extra synchronisation): elapsed time is
+  // read at the update's selection sync, when both events have completed
+  bool timing = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double jac_ms = 0.0, jac_flops = 0.0;
+  int64_t jac_launches = 0;
   int last_ns = 0;
   int64_t launches = 0;
   std::string err;
@@ -272,6 +284,10 @@ int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
   const int JBc = jacobi_block_cols();
   for (int s = 0; s < ns; ++s) {
     const SectorDesc& S = P.sd[s];
+    if (S.rows_tot > jacobi_max_rows())
+      return fail(h, BSMPO_ECAPACITY, "sector with " + std::to_string(S.rows_tot) +
+                                          " Jacobi rows exceeds the supported " +
+                                          std::to_string(jacobi_max_rows()));
     P.max_k = std::max(P.max_k, S.k);
     if (S.left) P.max_left_m2 = std::max(P.max_left_m2, S.m * S.m);
     JacobiWork w;
@@ -280,9 +296,17 @@ int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
     const int nbp = w.nblk + (w.nblk & 1);
     w.npairs = nbp / 2;
     w.rounds = nbp - 1;
+    // fewest CTAs per pair whose row share fits in shared memory (the redundant
+    // per-CTA Gram solve makes more CTAs per pair cost more in total)
+    w.cs = 1;
+    while (w.cs < jacobi_cluster_ctas() &&
+           ceil_div(ceil_div(S.rows_tot, w.cs), 16) * 16 > jacobi_rows_per_cta())
+      w.cs *= 2;
+    const int ppc = jacobi_cluster_ctas() / w.cs;
+    w.clusters = ceil_div(w.npairs, ppc);
     w.cta_start = ctas;
     w.pad_ = 0;
-    ctas += w.npairs;
+    ctas += w.clusters;
     P.max_rounds = std::max(P.max_rounds, w.rounds);
     P.jw.push_back(w);
   }
@@ -321,9 +345,26 @@ int check_mode(bsmpo_ctx* h, int mode) {
   return BSMPO_OK;
 }
 
+struct StageClock {
+  bsmpo_ctx* h;
+  std::chrono::steady_clock::time_point t0;
+  explicit StageClock(bsmpo_ctx* hh) : h(hh), t0(std::chrono::steady_clock::now()) {}
+  // stage i done: with profiling on, wait for the device and add the elapsed time
+  int mark(int i) {
+    if (!h->profile) return BSMPO_OK;
+    CK(h, cudaStreamSynchronize(h->stream));
+    auto t1 = std::chrono::steady_clock::now();
+    h->stage_ms[i] += std::chrono::duration<double, std::milli>(t1 - t0).count();
+    t0 = t1;
+    return BSMPO_OK;
+  }
+};
+
 int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   int rc = check_mode(h, mode);
   if (rc) return rc;
+  StageClock clk(h);
+  h->updates++;
   const int d = h->d, chi = h->chi, dd = d * d;
   cudaStream_t st = h->stream;
   Plan P;
@@ -341,6 +382,7 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   if ((rc = grow(h, h->keys, std::max<int64_t>(P.s_elems, 1) * sizeof(double)))) return rc;
   if ((rc = grow(h, h->perm, std::max<int64_t>(P.s_elems, 1) * sizeof(int)))) return rc;
   if ((rc = grow(h, h->rot, (size_t)3 * ns * sizeof(int)))) return rc;
+  if ((rc = grow(h, h->nf2, (size_t)ns * sizeof(double)))) return rc;
   if ((rc = grow(h, h->kept, (size_t)(ns + 1) * sizeof(int) + 64))) return rc;
   const TabLayout L = layout_of(P);
   if ((rc = grow(h, h->tab, L.total))) return rc;
@@ -365,15 +407,20 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   const JacobiWork* jw_d = reinterpret_cast<const JacobiWork*>(dt + L.jw);
   const int64_t chi2 = (int64_t)chi * chi;
 
+  if ((rc = clk.mark(0))) return rc;
   // 1. Theta_q = Glc[a, q] Gcr[q, b] for every valid triple
   CKL(h, launch_zgemm_grouped(h->gamma, h->gamma, h->theta.p, nullptr, gg_d, (int)P.gg.size(),
                               P.gemm_tiles, st));
+  if ((rc = clk.mark(1))) return rc;
   // 2. identity rows of [T^H; I] and the gate mix
   CKL(h, launch_identity_rows(sd_d, ns, P.max_left_m2, h->abuf.p, st));
   CKL(h, launch_mix_d(d, tab_d, tidx_d, td_d, sd_d, pairs_d, (int)P.pairs.size(), P.mix_tiles,
                       u3_dev, h->theta.p, h->lam + (size_t)(mode + 2) * chi, h->cbuf.p, h->abuf.p,
                       st));
+  if ((rc = clk.mark(2))) return rc;
   // 3. blocked one-sided Jacobi
+  double* nf2 = reinterpret_cast<double*>(h->nf2.p);
+  CKL(h, launch_sector_norms(sd_d, ns, h->abuf.p, nf2, st));
   CK(h, cudaMemsetAsync(h->rot.p, 0, (size_t)3 * ns * sizeof(int), st));
   int* hrot = reinterpret_cast<int*>(static_cast<char*>(h->hres.p) + 1024);
   int t = 0;
@@ -382,13 +429,15 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   for (const auto& w : P.jw) min_rounds = std::min(min_rounds, w.rounds);
   bool converged = false;
   int checks = 0;
+  std::vector<int> conv_at(ns, -1);
+  if (h->timing) CK(h, cudaEventRecord(h->ev0, st));
   while (t < t_max) {
     // run one sweep of the largest sector, then test convergence
     const int chunk = std::max(1, P.max_rounds);
     for (int i = 0; i < chunk && t < t_max; ++i, ++t) {
       // tol <= 0: per-sector default 4 eps sqrt(rows of the Gram), at least 8 eps
       CKL(h, launch_jacobi_round(sd_d, jw_d, (int)P.jw.size(), P.jac_ctas, t, h->abuf.p,
-                                 reinterpret_cast<int*>(h->rot.p), 0.0, MAX_SWEEPS, st));
+                                 reinterpret_cast<int*>(h->rot.p), nf2, 0.0, MAX_SWEEPS, st));
     }
     CK(h, cudaMemcpyAsync(hrot, h->rot.p, (size_t)3 * ns * sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(h, cudaStreamSynchronize(st));
@@ -397,13 +446,61 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
     for (int s = 0; s < ns; ++s) {
       const int R = P.jw[s].rounds;
       const int done = t / R;
-      if (done < 1 || hrot[3 * s + (done - 1) % 3] != 0) { all = false; break; }
+      if (done < 1 || hrot[3 * s + (done - 1) % 3] != 0) { all = false; continue; }
+      if (conv_at[s] < 0) conv_at[s] = done;
     }
     if (all) { converged = true; break; }
   }
+  if (h->timing) CK(h, cudaEventRecord(h->ev1, st));
   h->last_sweeps = t / std::max(1, P.max_rounds);
-  if (!converged) return fail(h, BSMPO_ECONVERGE, "Jacobi SVD did not converge");
-  CKL(h, launch_jacobi_finish(sd_d, ns, P.max_k, h->abuf.p, reinterpret_cast<double*>(h->sig.p),
+  h->jacobi_rounds += t;
+  if (h->timing) {
+    float ms = 0.f;
+    CK(h, cudaEventSynchronize(h->ev1));
+    CK(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->jac_ms += ms;
+    h->jac_launches += t;
+    // algorithmic flops of the executed sweeps: per block pair and round the pair
+    // Gram (rows_g) and the rotation (rows_tot) of 32 columns, 8 flops per complex MAC
+    for (int s = 0; s < ns; ++s) {
+      const SectorDesc& S = P.sd[s];
+      const double sweeps = conv_at[s] > 0 ? conv_at[s] : (double)t / P.jw[s].rounds;
+      const double cols = 2.0 * jacobi_block_cols();
+      h->jac_flops += sweeps * P.jw[s].rounds * P.jw[s].npairs * 8.0 * cols * cols *
+                      ((double)S.rows_g + S.rows_tot);
+    }
+  }
+  if ((rc = clk.mark(3))) return rc;
+  if (!converged) {
+    std::string msg = "Jacobi SVD did not converge (mode " + std::to_string(mode) + ")";
+    for (int s = 0; s < ns; ++s) {
+      const int R = P.jw[s].rounds, done = t / R;
+      if (done >= 1 && hrot[3 * s + (done - 1) % 3] == 0) continue;
+      const SectorDesc& S = P.sd[s];
+      msg += "; sector (" + std::to_string(S.cc0) + "," + std::to_string(S.cc1) + ") m=" +
+             std::to_string(S.m) + " n=" + std::to_string(S.n) + " sweeps=" + std::to_string(done) +
+             " rotations=" + std::to_string(hrot[3 * s + (done - 1 + 3) % 3]);
+      const char* dump = std::getenv("BSMPO_DEBUG_DUMP");
+      if (dump && dump[0]) {
+        // the sector's C (row-major m x n complex128) followed by Lambda_R of its columns
+        std::vector<cplx> hc((size_t)S.m * S.n);
+        CK(h, cudaMemcpy(hc.data(), static_cast<cplx*>(h->cbuf.p) + S.c_off,
+                         hc.size() * sizeof(cplx), cudaMemcpyDeviceToHost));
+        FILE* f = std::fopen(dump, "wb");
+        if (f) {
+          int hdr[4] = {S.m, S.n, S.cc0, S.cc1};
+          std::fwrite(hdr, sizeof(int), 4, f);
+          std::fwrite(hc.data(), sizeof(cplx), hc.size(), f);
+          std::fclose(f);
+        }
+        dump = nullptr;
+      }
+      break;
+    }
+    return fail(h, BSMPO_ECONVERGE, msg);
+  }
+  CKL(h, launch_jacobi_finish(sd_d, ns, P.max_k, h->abuf.p, nf2,
+                              reinterpret_cast<double*>(h->sig.p),
                               reinterpret_cast<int*>(h->perm.p), st));
   // 4. selection -> kept counts (the one host sync of the update)
   int* kept_d = reinterpret_cast<int*>(h->kept.p);
@@ -417,6 +514,7 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   CK(h, cudaMemcpyAsync(htw, trunc_d, sizeof(double), cudaMemcpyDeviceToHost, st));
   CK(h, cudaStreamSynchronize(st));
   const int total_kept = hk[ns];
+  if ((rc = clk.mark(4))) return rc;
   // 5. V and W = V^H C
   std::vector<GemmGroup> wg;
   int wtiles = 0, max_vm = 0;
@@ -450,12 +548,14 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   CKL(h, launch_zgemm_grouped(h->vbuf.p, h->cbuf.p, h->wbuf.p, nullptr,
                               reinterpret_cast<const GemmGroup*>(h->tab2.p), (int)wg.size(), wtiles,
                               st));
+  if ((rc = clk.mark(5))) return rc;
   // 6. scatter into Gamma[mode], Gamma[mode+1], Lambda / charge of bond mode+1
   CKL(h, launch_scatter(tab_d, sd_d, ns, total_kept, chi, h->charge + (size_t)mode * chi * 2,
                         h->charge + (size_t)(mode + 2) * chi * 2, h->vbuf.p, h->wbuf.p,
                         reinterpret_cast<double*>(h->sig.p), h->gamma + (size_t)mode * chi2,
                         h->gamma + (size_t)(mode + 1) * chi2, h->lam + (size_t)(mode + 1) * chi,
                         h->charge + (size_t)(mode + 1) * chi * 2, st));
+  if ((rc = clk.mark(6))) return rc;
   // algorithmic minimum bytes: read Glc, Gcr, write Gamma_L, Gamma_R (complex128)
   {
     double nl = 0, nc = 0, nr = 0;
@@ -603,6 +703,8 @@ int bsmpo_create(int n, int d, int chi, int flags, bsmpo_ctx** out) {
     return fail(nullptr, BSMPO_ENOMEM, "state allocation failed");
   }
   h->cnt.assign((size_t)(n + 1) * d * d, 0);
+  const char* prof = std::getenv("BSMPO_PROFILE");
+  h->profile = prof && prof[0] == '1';
   *out = h;
   return BSMPO_OK;
 }
@@ -612,10 +714,12 @@ int bsmpo_destroy(bsmpo_ctx* h) {
   cudaStreamSynchronize(h->stream);
   DevBuf* bufs[] = {&h->theta, &h->cbuf, &h->abuf, &h->wbuf, &h->vbuf, &h->sig, &h->keys,
                     &h->perm, &h->tab, &h->tab2, &h->rot, &h->kept, &h->u3, &h->m4,
-                    &h->env_l, &h->env_r, &h->part, &h->outv, &h->dims};
+                    &h->env_l, &h->env_r, &h->part, &h->outv, &h->dims, &h->nf2};
   for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
   HostStage* hs[] = {&h->stage, &h->stage2, &h->hres};
   for (HostStage* b : hs) if (b->p) cudaFreeHost(b->p);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
   cudaFree(h->gamma); cudaFree(h->lam); cudaFree(h->charge);
   delete h;
   return BSMPO_OK;
@@ -826,5 +930,33 @@ int bsmpo_bond_dims(const bsmpo_ctx* h, int* dims) {
 }
 
 int64_t bsmpo_kernel_launches(const bsmpo_ctx* h) { return h ? h->launches : 0; }
+
+int bsmpo_set_timing(bsmpo_ctx* h, int on) {
+  if (!h) return fail(nullptr, BSMPO_EINVAL, "null handle");
+  if (on && !h->ev0) {
+    CK(h, cudaEventCreate(&h->ev0));
+    CK(h, cudaEventCreate(&h->ev1));
+  }
+  h->timing = on != 0;
+  h->jac_ms = h->jac_flops = 0.0;
+  h->jac_launches = 0;
+  return BSMPO_OK;
+}
+
+int bsmpo_jacobi_timing(const bsmpo_ctx* h, double* ms, double* flops, int64_t* launches) {
+  if (!h) return fail(nullptr, BSMPO_EINVAL, "null handle");
+  if (ms) *ms = h->jac_ms;
+  if (flops) *flops = h->jac_flops;
+  if (launches) *launches = h->jac_launches;
+  return BSMPO_OK;
+}
+
+int bsmpo_stage_times(const bsmpo_ctx* h, double* ms, int n) {
+  if (!h || !ms || n < 10) return fail(nullptr, BSMPO_EINVAL, "bad argument");
+  for (int i = 0; i < 8; ++i) ms[i] = h->stage_ms[i];
+  ms[8] = (double)h->jacobi_rounds;
+  ms[9] = (double)h->updates;
+  return BSMPO_OK;
+}
 
 }  // extern "C"

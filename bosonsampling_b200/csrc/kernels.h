@@ -120,18 +120,30 @@ cudaError_t launch_phase(int d, int chi, double phi, const int* charge_l, const 
 struct JacobiWork {
   int sector;       // index into the SectorDesc array
   int nblk;         // column blocks
-  int npairs;       // CTAs per round (block pairs)
+  int npairs;       // block pairs per round
   int rounds;       // rounds per sweep
-  int cta_start;    // first flat CTA index of this sector
+  int cta_start;    // first cluster index of this sector
+  int cs;           // CTAs per block pair (rows split cs ways); a cluster holds 8/cs pairs
+  int clusters;     // clusters of this sector
   int pad_;
 };
+// CTAs per cluster and rows a CTA holds in shared memory
+int jacobi_cluster_ctas();
+int jacobi_rows_per_cta();
 int jacobi_block_cols();
 cudaError_t launch_jacobi_round(const SectorDesc* sd_dev, const JacobiWork* work_dev, int n_work,
-                                int total_ctas, int t, void* abuf, int* rot_count, double tol,
-                                int max_sweeps, cudaStream_t s);
-// Column norms, descending sort (ties by column index): sig[s_off..], perm[s_off..].
+                                int total_clusters, int t, void* abuf, int* rot_count,
+                                const double* nf2, double tol, int max_sweeps, cudaStream_t s);
+// Largest number of Jacobi-matrix rows (|L| + |R| or |L|) a sector may have.
+int jacobi_max_rows();
+// ||T_s||_F^2 of each sector's Jacobi matrix (Gram rows), fixed-order reduction.
+cudaError_t launch_sector_norms(const SectorDesc* sd_dev, int n_sectors, const void* abuf,
+                                double* nf2, cudaStream_t s);
+// Column norms (0 below the numerical-rank floor), descending sort (ties by column
+// index): sig[s_off..], perm[s_off..].
 cudaError_t launch_jacobi_finish(const SectorDesc* sd_dev, int n_sectors, int max_k,
-                                 const void* abuf, double* sig, int* perm, cudaStream_t s);
+                                 const void* abuf, const double* nf2, double* sig, int* perm,
+                                 cudaStream_t s);
 
 // ---------------------------------------------------------------- contract.cu
 // Standalone sector contraction with per-element charges (the update_MPO drop-in).

@@ -260,6 +260,8 @@ __global__ __launch_bounds__(SEL_NT) void select_kernel(const UpdateTables* __re
     if (own) kept = gt + kept_s[s];
     __syncthreads();
   }
+  // a kept vector needs its own singular value > 0 (the key may come from the partner)
+  if (own) kept = min(kept, count_gt(sig + off, k, 0.0));
   if (own) kept_s[s] = kept;
   __syncthreads();
   // a cut inside a degenerate swapped pair keeps neither member

@@ -252,3 +252,23 @@ class MPOSimulator:
 
     def kernel_launches(self):
         return int(self.L.bsmpo_kernel_launches(self.h))
+
+    def set_timing(self, on=True):
+        self._chk(self.L.bsmpo_set_timing(self.h, 1 if on else 0))
+
+    def jacobi_timing(self):
+        """(device ms, algorithmic flops, launches) of the Jacobi phase since set_timing()."""
+        ms, fl = np.zeros(1), np.zeros(1)
+        n = ctypes.c_int64()
+        self._chk(self.L.bsmpo_jacobi_timing(self.h, _capi.dptr(ms), _capi.dptr(fl), ctypes.byref(n)))
+        return float(ms[0]), float(fl[0]), int(n.value)
+
+    def stage_times(self):
+        """Per-stage milliseconds (only with BSMPO_PROFILE=1 at creation)."""
+        ms = np.zeros(10)
+        self._chk(self.L.bsmpo_stage_times(self.h, _capi.dptr(ms), 10))
+        names = ["plan", "theta_gemm", "mix", "jacobi", "select_sync", "v_w", "scatter", "unused"]
+        out = {k: float(v) for k, v in zip(names, ms[:8])}
+        out["jacobi_rounds"] = int(ms[8])
+        out["updates"] = int(ms[9])
+        return out

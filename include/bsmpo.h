@@ -139,6 +139,21 @@ int bsmpo_bond_dims(const bsmpo_ctx* h, int* dims);
 /* Number of kernels this handle has launched since creation. */
 int64_t bsmpo_kernel_launches(const bsmpo_ctx* h);
 
+/* Time the Jacobi SVD phase of every update with CUDA events on the handle's stream
+ * (on != 0 enables and resets the counters; no extra synchronisation is added). */
+int bsmpo_set_timing(bsmpo_ctx* h, int on);
+
+/* Accumulated Jacobi-phase device time (ms), its algorithmic flops (executed sweeps:
+ * pair Gram + rotation of each 32-column block pair, 8 flops per complex MAC) and
+ * the number of Jacobi round launches since bsmpo_set_timing(h, 1). */
+int bsmpo_jacobi_timing(const bsmpo_ctx* h, double* ms, double* flops, int64_t* launches);
+
+/* Stage timing, filled only when the handle was created with BSMPO_PROFILE=1 in the
+ * environment (each stage then ends with a stream synchronisation).  ms[0..7]:
+ * plan+upload, Theta GEMM, mix, Jacobi rounds, finish+select+sync, V/W, scatter,
+ * (unused); ms[8] = Jacobi round launches, ms[9] = updates.  n >= 10. */
+int bsmpo_stage_times(const bsmpo_ctx* h, double* ms, int n);
+
 #ifdef __cplusplus
 }
 #endif

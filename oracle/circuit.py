@@ -29,7 +29,7 @@ def gate_tensors(bs_list, d):
     return [fock.update_tensor(interferometer.t_block(th, ph), d) for (_, _, th, ph) in bs_list]
 
 
-def run(n, eta, d, chi, seed, photon_modes=None, max_bs=None, infos=None, phases=True):
+def run(n, eta, d, chi, seed, photon_modes=None, max_bs=None, infos=None, phases=True, cutoff=0.0):
     """Run the mesh of the seeded Haar unitary; returns (state, U, bs_list)."""
     U, bs, ph = interferometer.circuit(n, seed)
     if photon_modes is None:
@@ -38,7 +38,7 @@ def run(n, eta, d, chi, seed, photon_modes=None, max_bs=None, infos=None, phases
     todo = bs if max_bs is None else bs[:max_bs]
     for (layer, m, th, phi) in todo:
         U3 = fock.update_tensor(interferometer.t_block(th, phi), d)
-        info = mpo.bs_update(st, m, U3)
+        info = mpo.bs_update(st, m, U3, cutoff=cutoff)
         if infos is not None:
             infos.append(info)
     if phases and max_bs is None:

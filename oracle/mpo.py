@@ -25,7 +25,11 @@ Deliberate, documented differences from the reference's ``InitializationMPO.Upda
 3. the new bond is stored sorted by charge (the GPU driver's lexsort,
    ``src/beam_splitter_parallel/Rank.py:182-196``), empty slots get the sentinel d;
 4. only singular values > 0 are candidates -- the reference keeps exact zeros but then
-   masks them out everywhere through Lambda > 0 (``src/MPO.py:184-188``).
+   masks them out everywhere through Lambda > 0 (``src/MPO.py:184-188``);
+5. singular values at or below the numerical-rank floor 16 eps sqrt(max(m, n))
+   ||theta||_F count as exact zeros: they are rounding noise of a rank-deficient
+   sector, whose singular vectors are arbitrary (the reference, in complex64, keeps
+   such noise vectors as bond entries).
 """
 from dataclasses import dataclass, field
 
@@ -191,7 +195,7 @@ def selection_keys(sectors, sigmas):
     return keys
 
 
-def select_top(sectors, keys, chi):
+def select_top(sectors, keys, chi, thr=0.0, sigmas=None):
     """Deterministic top-chi: returns kept count per sector (a prefix of each sector).
 
     Entries are ranked by key (descending), then sector loop order, then in-sector
@@ -201,12 +205,15 @@ def select_top(sectors, keys, chi):
     entries = []
     for s, k in enumerate(keys):
         for i, v in enumerate(k):
-            if v > 0:
+            if v > thr and v > 0:
                 entries.append((-float(v), s, i))
     entries.sort()
     kept = [0] * len(keys)
     for (_, s, i) in entries[:chi]:
         kept[s] = max(kept[s], i + 1)
+    if sigmas is not None:
+        # a kept vector needs its own singular value > 0 (the key may be the partner's)
+        kept = [min(k, int(np.sum(sg > 0))) for k, sg in zip(kept, sigmas)]
     pos = {sec: i for i, sec in enumerate(sectors)}
     for s, (x, y) in enumerate(sectors):
         j = pos.get((y, x))
@@ -216,14 +223,15 @@ def select_top(sectors, keys, chi):
     return kept
 
 
-def bs_update(st, mode, U3, info=None):
+def bs_update(st, mode, U3, info=None, cutoff=0.0):
     """Apply the two-site gate with tensor ``U3[new_a, new_b, old_a]`` on (mode, mode+1).
 
     Restates ``InitializationMPO.Update`` (``src/MPO.py:158-303``): per new centre charge
     (cc0, cc1) the block product ``Gamma_L[a, q] diag(U (x) U*) Gamma_R[q, b]`` over valid
     charge triples a >= q >= b (``src/MPO.py:234-254``), ``theta = C diag(Lambda_R)``
     (``:256``), thin SVD (``:258``), ``W = V^H C`` (``:261``), top-chi truncation
-    (``:272-279``) and scatter (``:286-303``).
+    (``:272-279``) and scatter (``:286-303``).  ``cutoff`` > 0 additionally drops
+    singular values <= cutoff * (largest singular value of the update).
     """
     d, chi, n = st.d, st.chi, st.n
     CL, CC, CR = st.charge[mode], st.charge[mode + 1], st.charge[mode + 2]
@@ -269,6 +277,10 @@ def bs_update(st, mode, U3, info=None):
                 lo += len(la)
             theta = C * LR[r_bond][None, :]
             V, s, _ = np.linalg.svd(theta, full_matrices=False)
+            # numerical rank: singular values <= 16 eps sqrt(max(m, n)) ||theta||_F are
+            # rounding noise of a rank-deficient block and count as exact zeros
+            floor = 16.0 * np.finfo(np.float64).eps * np.sqrt(max(theta.shape)) * np.linalg.norm(theta)
+            s = np.where(s <= floor, 0.0, s)
             W = np.conj(V.T) @ C
             info.sectors.append((cc0, cc1))
             info.sigma.append(s)
@@ -278,7 +290,8 @@ def bs_update(st, mode, U3, info=None):
             sec_l.append(l_bond)
             sec_r.append(r_bond)
     keys = selection_keys(info.sectors, info.sigma)
-    kept = select_top(info.sectors, keys, chi)
+    smax = max([float(x[0]) for x in info.sigma if len(x)] + [0.0])
+    kept = select_top(info.sectors, keys, chi, cutoff * smax, info.sigma)
     info.kept = kept
     info.trunc_weight = float(sum(float(np.sum(s[k:] ** 2)) for s, k in zip(info.sigma, kept)))
     # scatter in sector (= charge) order, each sector's kept prefix in sigma order

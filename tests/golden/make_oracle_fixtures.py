@@ -1,0 +1,43 @@
+"""Generate oracle fixtures for the full seeded workloads (CPU, no GPU needed).
+
+    python tests/golden/make_oracle_fixtures.py [plain-small] [plain-scale]
+
+Runs the CPU oracle (oracle/) over the whole Clements mesh of each workload and
+stores the final trace, single-mode marginals, per-bond Lambda spectra (with their
+charges) and the per-update truncation weights, so GPU parity tests at these sizes
+do not have to rerun the oracle (the 496-update workload takes minutes on a CPU).
+"""
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import circuit, mpo  # noqa: E402
+
+
+def main(names):
+    for name in names:
+        w = circuit.WORKLOADS[name]
+        t0 = time.time()
+        infos = []
+        st, U, bs = circuit.run(**w, infos=infos)
+        P = mpo.marginals(st)
+        out = dict(
+            n=w["n"], eta=w["eta"], d=w["d"], chi=w["chi"], seed=w["seed"],
+            trace=np.array([mpo.trace(st)]), marginals=P,
+            lam=st.Lambda, charge=st.charge,
+            trunc_weight=np.array([i.trunc_weight for i in infos]),
+            bond_dims=np.array(mpo.bond_dims(st)),
+        )
+        path = os.path.join(HERE, "oracle_%s.npz" % name.replace("-", "_"))
+        np.savez_compressed(path, **out)
+        print(name, "%.1f s" % (time.time() - t0), "trace", out["trace"][0], "->", path,
+              os.path.getsize(path), "bytes")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:] or ["plain-small", "plain-scale"])
