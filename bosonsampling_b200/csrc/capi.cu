@@ -43,6 +43,8 @@ size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 }  // namespace
 
+void set_global_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
 struct bsmpo_ctx {
   int n = 0, d = 0, chi = 0;
   int device = 0;

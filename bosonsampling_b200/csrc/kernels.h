@@ -4,6 +4,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/bsmpo.h"
+
+// Message returned by bsmpo_last_error(NULL) (capi.cu).
+void set_global_error(const char* msg);
+
 // Largest local cutoff d supported (charge tables are d x d).
 #define BSMPO_MAX_D 8
 #define BSMPO_MAX_Q (BSMPO_MAX_D * BSMPO_MAX_D)

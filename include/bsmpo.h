@@ -154,6 +154,28 @@ int bsmpo_jacobi_timing(const bsmpo_ctx* h, double* ms, double* flops, int64_t* 
  * (unused); ms[8] = Jacobi round launches, ms[9] = updates.  n >= 10. */
 int bsmpo_stage_times(const bsmpo_ctx* h, double* ms, int n);
 
+/* Largest bond dimension bsmpo_trace_noalloc accepts. */
+#define BSMPO_NOALLOC_MAX_CHI 4096
+
+/* MPO trace without any device allocation.  No counterpart in the reference: it is
+ * for callers that cannot call cudaMalloc -- code running under a framework that owns
+ * all device memory (a caching allocator that must see every allocation), or a hook
+ * between beam-splitter updates that must not incur an allocation's implicit device
+ * synchronisation.  Computes the same trace as bsmpo_observables from caller-owned
+ * device buffers in the state layout above (gamma [n][chi][chi] complex128, lambda
+ * [n-1][chi], charge [n+1][chi][2]); writes (re, im) to the device buffer trace_out
+ * (2 doubles), on `stream`.  Its scratch is a fixed array inside the library,
+ * 2 * BSMPO_NOALLOC_MAX_CHI + 256 complex128 entries (about 135 KB) that every GPU
+ * loading the library keeps until the process exits; chi > BSMPO_NOALLOC_MAX_CHI is
+ * rejected with BSMPO_EINVAL.  The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress, with the device current), so make the first
+ * call on each device before any stream capture.  All calls share the array, and
+ * every call rewrites all of the scratch it reads: calls that overlap on the GPU
+ * (other streams, other host threads) race; serialise them.  Errors: see
+ * bsmpo_last_error(NULL). */
+int bsmpo_trace_noalloc(int n, int d, int chi, const void* gamma, const double* lambda,
+                        const int* charge, double* trace_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
