@@ -59,7 +59,7 @@ struct bsmpo_ctx {
   std::vector<int> cnt;
   // workspaces
   DevBuf theta, cbuf, abuf, wbuf, vbuf, sig, keys, perm, tab, tab2, rot, kept, u3, m4, env_l,
-      env_r, part, outv, dims, nf2;
+      env_r, part, outv, dims, nf2, qbuf, qflag;
   HostStage stage, stage2, hres;
   // last update diagnostics (host)
   std::vector<int> last_cc, last_shape, last_kept, last_k;
@@ -70,6 +70,7 @@ struct bsmpo_ctx {
   bool profile = false;
   double stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int64_t jacobi_rounds = 0, updates = 0;
+  int jac_rows = 128;  // target rows per CTA in a Jacobi round (BSMPO_JACOBI_ROWS)
   // Jacobi-phase timing with CUDA events (no extra synchronisation): elapsed time is
   // read at the update's selection sync, when both events have completed
   bool timing = false;
@@ -298,11 +299,12 @@ int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
     const int nbp = w.nblk + (w.nblk & 1);
     w.npairs = nbp / 2;
     w.rounds = nbp - 1;
-    // fewest CTAs per pair whose row share fits in shared memory (the redundant
-    // per-CTA Gram solve makes more CTAs per pair cost more in total)
+    // CTAs per pair: enough that each CTA's row share is at most h->jac_rows (the
+    // round's latency is set by the largest pair), and at least enough to fit
     w.cs = 1;
     while (w.cs < jacobi_cluster_ctas() &&
-           ceil_div(ceil_div(S.rows_tot, w.cs), 16) * 16 > jacobi_rows_per_cta())
+           (ceil_div(ceil_div(S.rows_tot, w.cs), 16) * 16 > jacobi_rows_per_cta() ||
+            ceil_div(S.rows_tot, w.cs) > h->jac_rows))
       w.cs *= 2;
     const int ppc = jacobi_cluster_ctas() / w.cs;
     w.clusters = ceil_div(w.npairs, ppc);
@@ -385,6 +387,9 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   if ((rc = grow(h, h->perm, std::max<int64_t>(P.s_elems, 1) * sizeof(int)))) return rc;
   if ((rc = grow(h, h->rot, (size_t)3 * ns * sizeof(int)))) return rc;
   if ((rc = grow(h, h->nf2, (size_t)ns * sizeof(double)))) return rc;
+  const int qslots = jacobi_qslots(P.jac_ctas);
+  if ((rc = grow(h, h->qbuf, (size_t)qslots * 32 * 32 * sizeof(cplx)))) return rc;
+  if ((rc = grow(h, h->qflag, (size_t)qslots * sizeof(int)))) return rc;
   if ((rc = grow(h, h->kept, (size_t)(ns + 1) * sizeof(int) + 64))) return rc;
   const TabLayout L = layout_of(P);
   if ((rc = grow(h, h->tab, L.total))) return rc;
@@ -438,8 +443,10 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
     const int chunk = std::max(1, P.max_rounds);
     for (int i = 0; i < chunk && t < t_max; ++i, ++t) {
       // tol <= 0: per-sector default 4 eps sqrt(rows of the Gram), at least 8 eps
-      CKL(h, launch_jacobi_round(sd_d, jw_d, (int)P.jw.size(), P.jac_ctas, t, h->abuf.p,
-                                 reinterpret_cast<int*>(h->rot.p), nf2, 0.0, MAX_SWEEPS, st));
+      CK(h, launch_jacobi_round(sd_d, jw_d, (int)P.jw.size(), P.jac_ctas, t, h->abuf.p,
+                                reinterpret_cast<int*>(h->rot.p), nf2, 0.0, MAX_SWEEPS, h->qbuf.p,
+                                reinterpret_cast<int*>(h->qflag.p), st));
+      h->launches += 2;
     }
     CK(h, cudaMemcpyAsync(hrot, h->rot.p, (size_t)3 * ns * sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(h, cudaStreamSynchronize(st));
@@ -707,6 +714,8 @@ int bsmpo_create(int n, int d, int chi, int flags, bsmpo_ctx** out) {
   h->cnt.assign((size_t)(n + 1) * d * d, 0);
   const char* prof = std::getenv("BSMPO_PROFILE");
   h->profile = prof && prof[0] == '1';
+  const char* jr = std::getenv("BSMPO_JACOBI_ROWS");
+  if (jr && std::atoi(jr) >= 16) h->jac_rows = std::atoi(jr);
   *out = h;
   return BSMPO_OK;
 }
@@ -716,7 +725,8 @@ int bsmpo_destroy(bsmpo_ctx* h) {
   cudaStreamSynchronize(h->stream);
   DevBuf* bufs[] = {&h->theta, &h->cbuf, &h->abuf, &h->wbuf, &h->vbuf, &h->sig, &h->keys,
                     &h->perm, &h->tab, &h->tab2, &h->rot, &h->kept, &h->u3, &h->m4,
-                    &h->env_l, &h->env_r, &h->part, &h->outv, &h->dims, &h->nf2};
+                    &h->env_l, &h->env_r, &h->part, &h->outv, &h->dims, &h->nf2, &h->qbuf,
+                    &h->qflag};
   for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
   HostStage* hs[] = {&h->stage, &h->stage2, &h->hres};
   for (HostStage* b : hs) if (b->p) cudaFreeHost(b->p);

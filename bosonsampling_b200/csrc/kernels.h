@@ -136,9 +136,14 @@ struct JacobiWork {
 int jacobi_cluster_ctas();
 int jacobi_rows_per_cta();
 int jacobi_block_cols();
+// Two launches: the pair Gram + test + inner Jacobi sweep (clusters), then the rotation
+// of every pair's rows.  qbuf holds jacobi_qslots(total_clusters) 32 x 32 complex
+// rotations, qflag as many ints.
 cudaError_t launch_jacobi_round(const SectorDesc* sd_dev, const JacobiWork* work_dev, int n_work,
                                 int total_clusters, int t, void* abuf, int* rot_count,
-                                const double* nf2, double tol, int max_sweeps, cudaStream_t s);
+                                const double* nf2, double tol, int max_sweeps, void* qbuf,
+                                int* qflag, cudaStream_t s);
+int jacobi_qslots(int total_clusters);
 // Largest number of Jacobi-matrix rows (|L| + |R| or |L|) a sector may have.
 int jacobi_max_rows();
 // ||T_s||_F^2 of each sector's Jacobi matrix (Gram rows), fixed-order reduction.
