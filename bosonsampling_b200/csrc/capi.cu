@@ -59,7 +59,7 @@ struct bsmpo_ctx {
   std::vector<int> cnt;
   // workspaces
   DevBuf theta, cbuf, abuf, wbuf, vbuf, sig, keys, perm, tab, tab2, rot, kept, u3, m4, env_l,
-      env_r, part, outv, dims, nf2, qbuf, qflag;
+      env_r, part, outv, dims, nf2, qbuf, qflag, pbuf, pcnt;
   HostStage stage, stage2, hres;
   // last update diagnostics (host)
   std::vector<int> last_cc, last_shape, last_kept, last_k;
@@ -70,7 +70,7 @@ struct bsmpo_ctx {
   bool profile = false;
   double stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int64_t jacobi_rounds = 0, updates = 0;
-  int jac_rows = 128;  // target rows per CTA in a Jacobi round (BSMPO_JACOBI_ROWS)
+  int jac_rows = 128;  // rows per part of a block pair in a Jacobi round (BSMPO_JACOBI_ROWS)
   // Jacobi-phase timing with CUDA events (no extra synchronisation): elapsed time is
   // read at the update's selection sync, when both events have completed
   bool timing = false;
@@ -145,10 +145,32 @@ struct Plan {
   std::vector<MixPair> pairs;
   std::vector<GemmGroup> gg;
   std::vector<JacobiWork> jw;
-  int mix_tiles = 0, gemm_tiles = 0, jac_ctas = 0, max_rounds = 0, max_k = 0, max_left_m2 = 0;
+  int mix_tiles = 0, gemm_tiles = 0, max_rounds = 0, max_k = 0, max_left_m2 = 0;
+  int gram_ctas = 0, apply_ctas = 0, jac_slots = 0;   // every sector in one round
   int64_t theta_elems = 0, c_elems = 0, a_elems = 0, s_elems = 0, w_elems = 0, v_elems = 0;
   double flops_theta = 0.0;
 };
+
+// Orders a round's work entries (most rounds per sweep first: those sectors set the
+// length of the Jacobi phase, so their CTAs are dispatched first) and assigns their
+// CTA ranges and block-pair slots.
+void jacobi_launch_list(std::vector<JacobiWork>& w, int* gram_ctas, int* apply_ctas, int* slots) {
+  std::stable_sort(w.begin(), w.end(), [](const JacobiWork& a, const JacobiWork& b) {
+    return a.rounds * a.npairs * a.cs > b.rounds * b.npairs * b.cs;
+  });
+  int g = 0, a = 0, sl = 0;
+  for (auto& x : w) {
+    x.gram_start = g;
+    x.apply_start = a;
+    x.slot_start = sl;
+    g += x.npairs * x.cs_g;
+    a += x.npairs * x.cs;
+    sl += x.npairs;
+  }
+  *gram_ctas = g;
+  *apply_ctas = a;
+  *slots = sl;
+}
 
 int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
   const int d = h->d, dd = d * d;
@@ -280,41 +302,33 @@ int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
   T.n_pairs = (int)P.pairs.size();
   // Jacobi work
   P.jw.clear();
-  int ctas = 0;
   P.max_rounds = 0;
   P.max_k = 0;
   P.max_left_m2 = 0;
   const int JBc = jacobi_block_cols();
+  const int rmax = std::min(h->jac_rows, jacobi_rows_per_part());
   for (int s = 0; s < ns; ++s) {
     const SectorDesc& S = P.sd[s];
-    if (S.rows_tot > jacobi_max_rows())
-      return fail(h, BSMPO_ECAPACITY, "sector with " + std::to_string(S.rows_tot) +
-                                          " Jacobi rows exceeds the supported " +
-                                          std::to_string(jacobi_max_rows()));
     P.max_k = std::max(P.max_k, S.k);
     if (S.left) P.max_left_m2 = std::max(P.max_left_m2, S.m * S.m);
     JacobiWork w;
+    std::memset(&w, 0, sizeof(w));
     w.sector = s;
     w.nblk = ceil_div(S.k, JBc);
     const int nbp = w.nblk + (w.nblk & 1);
     w.npairs = nbp / 2;
     w.rounds = nbp - 1;
-    // CTAs per pair: enough that each CTA's row share is at most h->jac_rows (the
-    // round's latency is set by the largest pair), and at least enough to fit
-    w.cs = 1;
-    while (w.cs < jacobi_cluster_ctas() &&
-           (ceil_div(ceil_div(S.rows_tot, w.cs), 16) * 16 > jacobi_rows_per_cta() ||
-            ceil_div(S.rows_tot, w.cs) > h->jac_rows))
-      w.cs *= 2;
-    const int ppc = jacobi_cluster_ctas() / w.cs;
-    w.clusters = ceil_div(w.npairs, ppc);
-    w.cta_start = ctas;
-    w.pad_ = 0;
-    ctas += w.clusters;
+    // parts of at most rmax rows (multiples of 16), as even as that allows; every part
+    // is non-empty, and the first cs_g hold the Gram rows
+    const int cs0 = ceil_div(S.rows_tot, rmax);
+    w.chunk = ceil_div(ceil_div(S.rows_tot, cs0), 16) * 16;
+    w.cs = ceil_div(S.rows_tot, w.chunk);
+    w.cs_g = ceil_div(S.rows_g, w.chunk);
     P.max_rounds = std::max(P.max_rounds, w.rounds);
     P.jw.push_back(w);
   }
-  P.jac_ctas = ctas;
+  std::vector<JacobiWork> all(P.jw);
+  jacobi_launch_list(all, &P.gram_ctas, &P.apply_ctas, &P.jac_slots);
   return BSMPO_OK;
 }
 
@@ -387,9 +401,11 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   if ((rc = grow(h, h->perm, std::max<int64_t>(P.s_elems, 1) * sizeof(int)))) return rc;
   if ((rc = grow(h, h->rot, (size_t)3 * ns * sizeof(int)))) return rc;
   if ((rc = grow(h, h->nf2, (size_t)ns * sizeof(double)))) return rc;
-  const int qslots = jacobi_qslots(P.jac_ctas);
-  if ((rc = grow(h, h->qbuf, (size_t)qslots * 32 * 32 * sizeof(cplx)))) return rc;
-  if ((rc = grow(h, h->qflag, (size_t)qslots * sizeof(int)))) return rc;
+  const size_t pair_elems = (size_t)4 * jacobi_block_cols() * jacobi_block_cols();
+  if ((rc = grow(h, h->qbuf, std::max(P.jac_slots, 1) * pair_elems * sizeof(cplx)))) return rc;
+  if ((rc = grow(h, h->qflag, std::max(P.jac_slots, 1) * sizeof(int)))) return rc;
+  if ((rc = grow(h, h->pcnt, std::max(P.jac_slots, 1) * sizeof(int)))) return rc;
+  if ((rc = grow(h, h->pbuf, std::max(P.gram_ctas, 1) * pair_elems * sizeof(cplx)))) return rc;
   if ((rc = grow(h, h->kept, (size_t)(ns + 1) * sizeof(int) + 64))) return rc;
   const TabLayout L = layout_of(P);
   if ((rc = grow(h, h->tab, L.total))) return rc;
@@ -402,7 +418,10 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   put(hs, L.sd, P.sd);
   put(hs, L.pairs, P.pairs);
   put(hs, L.gg, P.gg);
-  put(hs, L.jw, P.jw);
+  std::vector<JacobiWork> active(P.jw);
+  int gram_ctas = 0, apply_ctas = 0, slots = 0;
+  jacobi_launch_list(active, &gram_ctas, &apply_ctas, &slots);
+  put(hs, L.jw, active);
   char* dt = static_cast<char*>(h->tab.p);
   CK(h, cudaMemcpyAsync(dt, hs, L.total, cudaMemcpyHostToDevice, st));
   const UpdateTables* tab_d = reinterpret_cast<const UpdateTables*>(dt + L.tab);
@@ -429,11 +448,10 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   double* nf2 = reinterpret_cast<double*>(h->nf2.p);
   CKL(h, launch_sector_norms(sd_d, ns, h->abuf.p, nf2, st));
   CK(h, cudaMemsetAsync(h->rot.p, 0, (size_t)3 * ns * sizeof(int), st));
+  CK(h, cudaMemsetAsync(h->pcnt.p, 0, std::max(P.jac_slots, 1) * sizeof(int), st));
   int* hrot = reinterpret_cast<int*>(static_cast<char*>(h->hres.p) + 1024);
   int t = 0;
   const int t_max = MAX_SWEEPS * std::max(1, P.max_rounds);
-  int min_rounds = P.max_rounds;
-  for (const auto& w : P.jw) min_rounds = std::min(min_rounds, w.rounds);
   bool converged = false;
   int checks = 0;
   std::vector<int> conv_at(ns, -1);
@@ -443,8 +461,9 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
     const int chunk = std::max(1, P.max_rounds);
     for (int i = 0; i < chunk && t < t_max; ++i, ++t) {
       // tol <= 0: per-sector default 4 eps sqrt(rows of the Gram), at least 8 eps
-      CK(h, launch_jacobi_round(sd_d, jw_d, (int)P.jw.size(), P.jac_ctas, t, h->abuf.p,
-                                reinterpret_cast<int*>(h->rot.p), nf2, 0.0, MAX_SWEEPS, h->qbuf.p,
+      CK(h, launch_jacobi_round(sd_d, jw_d, (int)active.size(), gram_ctas, apply_ctas, t,
+                                h->abuf.p, reinterpret_cast<int*>(h->rot.p), nf2, 0.0, MAX_SWEEPS,
+                                h->pbuf.p, reinterpret_cast<int*>(h->pcnt.p), h->qbuf.p,
                                 reinterpret_cast<int*>(h->qflag.p), st));
       h->launches += 2;
     }
@@ -453,12 +472,26 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
     ++checks;
     bool all = true;
     for (int s = 0; s < ns; ++s) {
+      // a converged sector leaves the launches, and its counters are stale from then on
+      if (conv_at[s] >= 0) continue;
       const int R = P.jw[s].rounds;
       const int done = t / R;
       if (done < 1 || hrot[3 * s + (done - 1) % 3] != 0) { all = false; continue; }
-      if (conv_at[s] < 0) conv_at[s] = done;
+      conv_at[s] = done;
     }
     if (all) { converged = true; break; }
+    // drop converged sectors (and those out of sweeps) from the next rounds' launches;
+    // the stream is idle, so the pinned stage and the device table are free
+    std::vector<JacobiWork> next;
+    for (const auto& w : P.jw)
+      if (conv_at[w.sector] < 0 && t / w.rounds < MAX_SWEEPS) next.push_back(w);
+    if (next.size() < active.size() && !next.empty()) {
+      active.swap(next);
+      jacobi_launch_list(active, &gram_ctas, &apply_ctas, &slots);
+      put(hs, L.jw, active);
+      CK(h, cudaMemcpyAsync(dt + L.jw, hs + L.jw, active.size() * sizeof(JacobiWork),
+                            cudaMemcpyHostToDevice, st));
+    }
   }
   if (h->timing) CK(h, cudaEventRecord(h->ev1, st));
   h->last_sweeps = t / std::max(1, P.max_rounds);
@@ -484,7 +517,7 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
     std::string msg = "Jacobi SVD did not converge (mode " + std::to_string(mode) + ")";
     for (int s = 0; s < ns; ++s) {
       const int R = P.jw[s].rounds, done = t / R;
-      if (done >= 1 && hrot[3 * s + (done - 1) % 3] == 0) continue;
+      if (conv_at[s] >= 0) continue;
       const SectorDesc& S = P.sd[s];
       msg += "; sector (" + std::to_string(S.cc0) + "," + std::to_string(S.cc1) + ") m=" +
              std::to_string(S.m) + " n=" + std::to_string(S.n) + " sweeps=" + std::to_string(done) +

@@ -4,28 +4,23 @@
 // Rank.py:123) / LAPACK svd (src/MPO.py:258).  The Jacobi matrix of a sector is
 // T = C diag(Lambda_R) when |L| >= |R| (its orthogonalised columns are sigma * V),
 // or [T^H; I] when |L| < |R| (the identity rows accumulate V).  Columns are cut in
-// blocks of 16; a round pairs the blocks by the circle method, and one CTA per block
-// pair is split over 1-16 CTAs of a 16-CTA thread-block cluster by rows (all
-// sectors of the update in one launch; small pairs share a cluster):
-//   1. each CTA loads its rows of the pair's 32 columns into shared memory and forms
-//      a partial 32 x 32 Gram; the partials are summed through distributed shared
-//      memory in a fixed order, so every CTA holds the same bit-exact Gram,
-//   2. the cluster stops if every pair is orthogonal to `tol` (relative), else
-//   3. every CTA runs the same cyclic two-sided Jacobi sweep on that Gram (complex
-//      rotations, 16 disjoint pairs per step), accumulating the 32 x 32 unitary Q, and
-//   4. applies Q to its own rows, writing them back to global memory.
+// blocks of 16; a round pairs the blocks by the circle method (all sectors of the
+// update in one launch pair), and each block pair's rows are cut in parts of at most
+// 128 rows:
+//   1. (gram kernel) every part holding Gram rows forms its partial 32 x 32 Gram; the
+//      last part to finish sums the partials in part order, tests the pair and, if a
+//      column pair is not orthogonal to `tol` (relative), runs one cyclic two-sided
+//      Jacobi sweep on the Gram (complex rotations, 16 disjoint pairs per step),
+//      accumulating the 32 x 32 unitary Q;
+//   2. (apply kernel) every part of a rotated pair applies Q to its rows.
 // A sector is converged after a sweep without rotations; later rounds of it exit
 // at once.  One-sided Jacobi keeps high relative accuracy for small singular values.
 // Numerical rank: a column whose norm is <= 16 eps sqrt(rows) ||T||_F is rounding
 // noise (the null space of a rank-deficient block); it takes part in no rotation and
 // its singular value is reported as 0, as is a column below tol times its partner
 // in a pair test.  Without this, noise columns never test orthogonal.
-#include <cooperative_groups.h>
-
 #include "common.cuh"
 #include "kernels.h"
-
-namespace cg = cooperative_groups;
 
 namespace {
 
@@ -40,71 +35,101 @@ __device__ __forceinline__ void dmma(double2& d, double a, double b) {
 constexpr int JB = 16;        // columns per block
 constexpr int JC = 2 * JB;    // columns per block pair
 constexpr int JNT = 256;
-constexpr int JCL = 16;       // CTAs per cluster (non-portable size, B200 supports 16)
-constexpr int RMAX = 128;     // rows per CTA held in shared memory (2 CTAs per SM)
+constexpr int RMAX = 128;     // rows of one part (Gram tile in shared memory)
 
-struct JacSmem {
-  double2 tile[RMAX][JC + 1];   // this CTA's rows of the pair's 32 columns
-  double2 G[JC][JC + 1];        // full pair Gram (identical in every CTA of the pair)
-  double2 Q[JC][JC + 1];        // partial Gram, then the accumulated rotation
-  double2 Gf[JC / 2][JC + 1];   // this CTA's slice of the reduced Gram (JC/cs rows, cs >= 2)
-  double rc[JC / 2];            // rotations of the current inner step
-  double2 rs[JC / 2];
-  int cols[JC];
-  JacobiWork W;
-  int64_t aoff;
-  int k, rows_g, rows_tot, rotate;
-  double z2;
-};
-
-// Where a CTA of a round works: its sector, block pair, row part and columns.
+// Where a CTA of a round works: its sector, block pair and row part.
 struct JacTask {
   JacobiWork W;
-  int pair, slot, part, cs, sweep, rr, valid, gslot;
+  int pair, part, sweep, rr, slot;
 };
 
-__device__ __forceinline__ JacTask jac_task(const JacobiWork* __restrict__ work, int n_work, int t) {
-  const int gc = blockIdx.x / JCL;
+// Gram launch: CTAs [gram_start, gram_start + npairs cs_g) of a work entry, pair-major;
+// apply launch: [apply_start, apply_start + npairs cs).
+__device__ __forceinline__ JacTask jac_task(const JacobiWork* __restrict__ work, int n_work, int t,
+                                            bool apply) {
+  const int b = blockIdx.x;
   int lo = 0, hi = n_work - 1;
   while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (work[mid].cta_start <= gc) lo = mid; else hi = mid - 1;
+    const int mid = (lo + hi + 1) >> 1;
+    const int st = apply ? work[mid].apply_start : work[mid].gram_start;
+    if (st <= b) lo = mid; else hi = mid - 1;
   }
   JacTask T;
   T.W = work[lo];
-  const int cr = blockIdx.x % JCL;
-  T.cs = T.W.cs;
-  T.slot = cr / T.cs;
-  T.part = cr % T.cs;
-  T.pair = (gc - T.W.cta_start) * (JCL / T.cs) + T.slot;
-  T.valid = T.pair < T.W.npairs;
+  const int per = apply ? T.W.cs : T.W.cs_g;
+  const int local = b - (apply ? T.W.apply_start : T.W.gram_start);
+  T.pair = local / per;
+  T.part = local % per;
   T.sweep = t / T.W.rounds;
   T.rr = t % T.W.rounds;
-  T.gslot = gc * JCL + T.slot * T.cs;   // one slot per block pair of the launch
+  T.slot = T.W.slot_start + T.pair;
   return T;
 }
 
-// the pair's 32 columns (-1: padding) for round rr of the circle method
+// circle method over n (even) positions: the item at position pos in step s; position 0
+// is fixed, the others turn by one place per step, pairs are (P, n - 1 - P)
+__device__ __forceinline__ int circle_at(int pos, int s, int n) {
+  return pos == 0 ? 0 : 1 + (pos - 1 + s) % (n - 1);
+}
+
+// the pair's c-th column (c < 16: first block, else second; -1: padding)
 __device__ __forceinline__ int jac_col(const JacTask& T, int c, int k) {
   const int nbp = T.W.nblk + (T.W.nblk & 1);
-  auto blk_at = [&](int pos) { return pos == 0 ? 0 : 1 + (pos - 1 + T.rr) % (nbp - 1); };
-  const int b = c < JB ? blk_at(T.pair) : blk_at(nbp - 1 - T.pair);
+  const int b = c < JB ? circle_at(T.pair, T.rr, nbp) : circle_at(nbp - 1 - T.pair, T.rr, nbp);
   const int col = b * JB + (c % JB);
-  return (T.valid && b < T.W.nblk && col < k) ? col : -1;
+  return (b < T.W.nblk && col < k) ? col : -1;
 }
 
-__device__ __forceinline__ void jac_rows(const JacTask& T, int rows_tot, int rows_g, int& r0, int& nr,
-                                         int& ng) {
-  const int chunk = ((rows_tot + T.cs - 1) / T.cs + 15) / 16 * 16;
-  r0 = T.part * chunk;
-  nr = T.valid ? max(0, min(rows_tot, r0 + chunk) - r0) : 0;
-  ng = T.valid ? max(0, min(rows_g, r0 + chunk) - r0) : 0;
+struct GramSmem {
+  union {
+    double2 tile[RMAX][JC + 1];   // this part's Gram rows of the pair's 32 columns
+    double2 G[JC][JC + 1];        // then the pair Gram (upper triangle, i <= j, is used)
+  } u;
+  double rc[JC / 2];              // rotations of the current inner step
+  double2 rs[JC / 2];
+  int cols[JC];
+  int rotate, last;
+  double z2;
+};
+
+// pair-Gram element (i, j) from the stored upper triangle
+__device__ __forceinline__ cplx gget(const GramSmem& S, int i, int j) {
+  if (i <= j) {
+    const double2 v = S.u.G[i][j];
+    return cmake(v.x, v.y);
+  }
+  const double2 v = S.u.G[j][i];
+  return cmake(v.x, -v.y);
 }
 
-// K1 of a round: pair Gram (rows split over cs CTAs of a cluster, reduced through
-// distributed shared memory in a fixed order), convergence test, and -- on the pair's
-// first CTA only -- one cyclic Jacobi sweep on the 32 x 32 Gram; Q and the rotate flag
-// go to global memory for K2.  The other CTAs of the pair leave after the reduction.
+__device__ __forceinline__ void gput(GramSmem& S, int i, int j, cplx v) {
+  if (i < j) S.u.G[i][j] = make_double2(v.x, v.y);
+  else S.u.G[j][i] = make_double2(v.x, -v.y);
+}
+
+// the ordered column pair (p < q) of pair P in inner step s
+__device__ __forceinline__ void inner_pq(int P, int s, int& p, int& q) {
+  p = circle_at(P, s, JC);
+  q = circle_at(JC - 1 - P, s, JC);
+  if (p > q) { const int x = p; p = q; q = x; }
+}
+
+// Round kernel 1: the pair Gram and, in the pair's last CTA to finish, the test and one
+// cyclic Jacobi sweep on it.
+//   a. every part (up to RMAX Gram rows) loads its rows of the pair's 32 columns and
+//      forms a partial Gram on the FP64 tensor path; with several parts the partials go
+//      to global memory and the last part to arrive (an arrival counter per pair) sums
+//      them in part order, so the Gram does not depend on arrival order;
+//   b. no rotation if every column pair is orthogonal to `tol` (relative); else
+//   c. a cyclic two-sided sweep (circle order, 16 disjoint rotations per step) on the
+//      Gram, accumulating the 32 x 32 unitary Q, which goes to global memory with a
+//      flag for the apply kernel.
+// The step's rotations are computed once (16 threads) and read by all; the Gram keeps
+// only its upper triangle; Q lives in registers in circle-position order -- thread
+// (pair L, rows g, g + 16) holds the entries of the two positions of pair L and passes
+// them to the neighbouring pairs by warp shuffles when the circle turns, so Q never
+// touches shared memory.  After the 31 steps the circle is back at its start and every
+// thread holds columns L and 31 - L.
 __global__ __launch_bounds__(JNT) void jacobi_gram_kernel(const SectorDesc* __restrict__ sd,
                                                           const JacobiWork* __restrict__ work,
                                                           int n_work, int t,
@@ -112,119 +137,126 @@ __global__ __launch_bounds__(JNT) void jacobi_gram_kernel(const SectorDesc* __re
                                                           int* __restrict__ rot_count,
                                                           const double* __restrict__ nf2,
                                                           double tol, int max_sweeps,
+                                                          cplx* __restrict__ pbuf,
+                                                          int* __restrict__ pcnt,
                                                           cplx* __restrict__ qbuf,
                                                           int* __restrict__ qflag) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  JacSmem& S = *reinterpret_cast<JacSmem*>(smem_raw);
-  cg::cluster_group cluster = cg::this_cluster();
+  GramSmem& S = *reinterpret_cast<GramSmem*>(smem_raw);
   const int tid = threadIdx.x;
-  const JacTask T = jac_task(work, n_work, t);
-  if (tid == 0) {
-    const SectorDesc& D = sd[T.W.sector];
-    S.k = D.k;
-    S.rows_g = D.rows_g;
-    S.rows_tot = D.rows_tot;
-    S.aoff = D.a_off;
-    // numerical-rank floor: columns with |a|^2 <= z2 are exact zeros for the SVD
-    const double zf = 16.0 * 2.220446049250313e-16 * sqrt((double)D.rows_g);
-    S.z2 = zf * zf * nf2[T.W.sector];
-    S.rotate = 0;
-  }
-  if (T.valid && T.part == 0 && tid == 0) qflag[T.gslot] = 0;
-  __syncthreads();
-  // every exit before the first cluster barrier depends on (sector, t) only, so the
-  // whole cluster takes it together
+  const JacTask T = jac_task(work, n_work, t, false);
+  if (T.part == 0 && tid == 0) qflag[T.slot] = 0;
+  // every exit before the arrival counter depends on (sector, t) only
   if (T.sweep >= max_sweeps) return;
   int* cnt = rot_count + 3 * T.W.sector;
   // the counter of sweep w+1 is cleared during sweep w (nobody else touches it then),
   // before the converged exit so that a converged sector keeps reading zeros
   if (T.rr == 0 && T.pair == 0 && T.part == 0 && tid == 0) cnt[(T.sweep + 1) % 3] = 0;
   if (T.sweep >= 1 && cnt[(T.sweep - 1) % 3] == 0) return;   // converged
-  const int k = S.k;
+  const SectorDesc& D = sd[T.W.sector];
+  const int k = D.k, rows_g = D.rows_g;
+  const int r0 = T.part * T.W.chunk;
+  const int ng = min(rows_g, r0 + T.W.chunk) - r0;   // >= 1: parts cover the Gram rows
   if (tid < JC) S.cols[tid] = jac_col(T, tid, k);
-  int r0, nr, ng;
-  jac_rows(T, S.rows_tot, S.rows_g, r0, nr, ng);
-  const int rows_g = S.rows_g;
-  const int cs = T.cs, part = T.part, sl = JC / cs, base = T.slot * cs;
-  const cplx* A = abuf + S.aoff;
+  if (tid == 0) {
+    // numerical-rank floor: columns with |a|^2 <= z2 are exact zeros for the SVD
+    const double zf = 16.0 * 2.220446049250313e-16 * sqrt((double)rows_g);
+    S.z2 = zf * zf * nf2[T.W.sector];
+    S.rotate = 0;
+  }
   __syncthreads();
 
-  // ---- 1. this CTA's rows -> shared memory; partial Gram over its Gram rows
-  for (int e = tid; e < ng * JC; e += JNT) {
-    const int r = e / JC, c = e % JC;
-    double2 v = make_double2(0.0, 0.0);
-    if (S.cols[c] >= 0) v = *reinterpret_cast<const double2*>(A + (int64_t)(r0 + r) * k + S.cols[c]);
-    S.tile[r][c] = v;
+  // ---- a. rows -> shared memory (all loads of a thread in flight), partial Gram
+  {
+    const cplx* A = abuf + D.a_off;
+    const int lane = tid & 31, wrow = tid >> 5;
+    const int col = S.cols[lane];
+    constexpr int PER = RMAX * JC / JNT;
+    double2 v[PER];
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int r = wrow + i * (JNT / JC);
+      v[i] = make_double2(0.0, 0.0);
+      if (r < ng && col >= 0) v[i] = *reinterpret_cast<const double2*>(A + (int64_t)(r0 + r) * k + col);
+    }
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int r = wrow + i * (JNT / JC);
+      if (r < ng) S.u.tile[r][lane] = v[i];
+    }
   }
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31, li = lane >> 2, lk = lane & 3;
-  {
-    // G[i][j] = sum_r conj(X[r][i]) X[r][j] on the FP64 tensor path: warp w owns the
-    // 8 x 8 tiles (I, J) = (w / 2, 2 (w % 2) + {0, 1}); rows in chunks of 4;
-    // (ar - i ai)(br + i bi) = (ar br + ai bi) + i (ar bi - ai br)
-    const int I = warp >> 1, J0 = 2 * (warp & 1);
-    double2 gre[2] = {make_double2(0, 0), make_double2(0, 0)};
-    double2 gim[2] = {make_double2(0, 0), make_double2(0, 0)};
-    for (int k0 = 0; k0 < ng; k0 += 4) {
-      const int r = k0 + lk;
-      const double2 a = r < ng ? S.tile[r][8 * I + li] : make_double2(0.0, 0.0);
-#pragma unroll
-      for (int jj = 0; jj < 2; ++jj) {
-        const double2 b = r < ng ? S.tile[r][8 * (J0 + jj) + li] : make_double2(0.0, 0.0);
-        dmma(gre[jj], a.x, b.x);
-        dmma(gre[jj], a.y, b.y);
-        dmma(gim[jj], a.x, b.y);
-        dmma(gim[jj], -a.y, b.x);
-      }
-    }
-    // the partial Gram lives in Q's storage until the rotation is accumulated there
+  // G[i][j] = sum_r conj(X[r][i]) X[r][j]: warp w owns the 8 x 8 tiles (I, J) =
+  // (w / 2, 2 (w % 2) + {0, 1}); rows in chunks of 4;
+  // (ar - i ai)(br + i bi) = (ar br + ai bi) + i (ar bi - ai br)
+  const int I = warp >> 1, J0 = 2 * (warp & 1);
+  double2 gre[2] = {make_double2(0, 0), make_double2(0, 0)};
+  double2 gim[2] = {make_double2(0, 0), make_double2(0, 0)};
+  for (int k0 = 0; k0 < ng; k0 += 4) {
+    const int r = k0 + lk;
+    const double2 a = r < ng ? S.u.tile[r][8 * I + li] : make_double2(0.0, 0.0);
 #pragma unroll
     for (int jj = 0; jj < 2; ++jj) {
-      const int row = 8 * I + li, col = 8 * (J0 + jj) + 2 * lk;
-      S.Q[row][col] = make_double2(gre[jj].x, gim[jj].x);
-      S.Q[row][col + 1] = make_double2(gre[jj].y, gim[jj].y);
+      const double2 b = r < ng ? S.u.tile[r][8 * (J0 + jj) + li] : make_double2(0.0, 0.0);
+      dmma(gre[jj], a.x, b.x);
+      dmma(gre[jj], a.y, b.y);
+      dmma(gim[jj], a.x, b.y);
+      dmma(gim[jj], -a.y, b.x);
     }
   }
-  cluster.sync();
-  // ---- 2. reduce: this CTA sums Gram rows [part*sl, part*sl + sl) over the pair's cs
-  //         CTAs, in rank order
-  if (T.valid && cs > 1) {
-    for (int e = tid; e < sl * JC; e += JNT) {
-      const int r = e / JC, c = e % JC;
+  __syncthreads();   // the tile is dead; G takes its place
+  const int cs_g = T.W.cs_g;
+  if (cs_g == 1) {
+#pragma unroll
+    for (int jj = 0; jj < 2; ++jj) {
+      const int row = 8 * I + li, c0 = 8 * (J0 + jj) + 2 * lk;
+      S.u.G[row][c0] = make_double2(gre[jj].x, gim[jj].x);
+      S.u.G[row][c0 + 1] = make_double2(gre[jj].y, gim[jj].y);
+    }
+  } else {
+    cplx* pp = pbuf + (int64_t)blockIdx.x * JC * JC;
+#pragma unroll
+    for (int jj = 0; jj < 2; ++jj) {
+      const int row = 8 * I + li, c0 = 8 * (J0 + jj) + 2 * lk;
+      __stcg(reinterpret_cast<double2*>(pp + row * JC + c0), make_double2(gre[jj].x, gim[jj].x));
+      __stcg(reinterpret_cast<double2*>(pp + row * JC + c0 + 1), make_double2(gre[jj].y, gim[jj].y));
+    }
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      const int old = atomicAdd(pcnt + T.slot, 1);
+      __threadfence();
+      S.last = (old == cs_g - 1);
+    }
+    __syncthreads();
+    if (!S.last) return;
+    // the last part: fixed-order sum of the upper triangles of the pair's partials
+    const cplx* p0 = pbuf + (int64_t)(blockIdx.x - T.part) * JC * JC;
+    for (int e = tid; e < JC * JC; e += JNT) {
+      const int i = e / JC, j = e % JC;
+      if (j < i) continue;
       double sx = 0.0, sy = 0.0;
-      for (int q = 0; q < cs; ++q) {
-        const JacSmem* R = cluster.map_shared_rank(&S, base + q);
-        const double2 v = R->Q[part * sl + r][c];
+#pragma unroll 4
+      for (int q = 0; q < cs_g; ++q) {
+        const double2 v = __ldcg(reinterpret_cast<const double2*>(p0 + (int64_t)q * JC * JC + e));
         sx += v.x;
         sy += v.y;
       }
-      S.Gf[r][c] = make_double2(sx, sy);
+      S.u.G[i][j] = make_double2(sx, sy);
     }
+    if (tid == 0) pcnt[T.slot] = 0;   // ready for the next round
   }
-  cluster.sync();
-  // ---- 3. the pair's first CTA gathers the reduced Gram
-  if (T.valid && part == 0) {
-    for (int e = tid; e < JC * JC; e += JNT) {
-      const int r = e / JC, c = e % JC;
-      if (cs == 1) {
-        S.G[r][c] = S.Q[r][c];
-      } else {
-        const JacSmem* R = cluster.map_shared_rank(&S, base + r / sl);
-        S.G[r][c] = R->Gf[r % sl][c];
-      }
-    }
-  }
-  cluster.sync();   // after this no CTA touches another CTA's shared memory
-  if (!(T.valid && part == 0)) return;
+  __syncthreads();
 
-  // ---- 4. convergence test (relative tolerance on |a_i^H a_j|)
+  // ---- b. convergence test (relative tolerance on |a_i^H a_j|)
   if (tol <= 0.0) tol = fmax(8.0 * 2.220446049250313e-16, 4.0 * 2.220446049250313e-16 * sqrt((double)rows_g));
   const double t2 = tol * tol, z2 = S.z2;
   for (int e = tid; e < JC * JC; e += JNT) {
     const int i = e / JC, j = e % JC;
     if (j <= i) continue;
-    const double dii = S.G[i][i].x, djj = S.G[j][j].x;
-    const double2 g = S.G[i][j];
+    const double dii = S.u.G[i][i].x, djj = S.u.G[j][j].x;
+    const double2 g = S.u.G[i][j];
     const double a2 = g.x * g.x + g.y * g.y;
     // a column at the numerical-rank floor, or below tol times its partner, is rounding
     // noise along the partner and is never rotated against it
@@ -234,11 +266,9 @@ __global__ __launch_bounds__(JNT) void jacobi_gram_kernel(const SectorDesc* __re
   if (!S.rotate) return;
   if (tid == 0) atomicAdd(cnt + T.sweep % 3, 1);
 
-  // ---- 5. one cyclic Jacobi sweep on the 32 x 32 Gram, accumulating Q.  A step rotates
-  //         16 disjoint column pairs: threads 0-15 compute the rotations while the others
-  //         fetch their operands; then G' = J^H G J, split into independent 2 x 2 blocks
-  //         J_P1^H G[P1][P2] J_P2 (upper block triangle + Hermitian mirror), and Q' = Q J.
-  for (int e = tid; e < JC * JC; e += JNT) S.Q[e / JC][e % JC] = make_double2((e / JC) == (e % JC) ? 1.0 : 0.0, 0.0);
+  // ---- c. one cyclic Jacobi sweep on the Gram
+  // block roles: thread < 136 updates the 2 x 2 block (P1, P2), P1 <= P2, of the pair
+  // positions; lanes 0-15 of the last warp compute the step's rotations
   int P1 = -1, P2 = -1;
   if (tid < (JC / 2) * (JC / 2 + 1) / 2) {
     int rem = tid;
@@ -246,21 +276,19 @@ __global__ __launch_bounds__(JNT) void jacobi_gram_kernel(const SectorDesc* __re
     while (rem >= JC / 2 - P1) { rem -= JC / 2 - P1; ++P1; }
     P2 = P1 + rem;
   }
-  const int qp = tid & 15, qr = tid >> 4;
-  __syncthreads();
+  const int rt = tid - (JNT - 32);
+  const int L = tid & 15, grp = tid >> 4;
+  // Q at step 0 is the identity: positions hold columns L (upper) and 31 - L (lower);
+  // rows grp < 16 meet column L only on the diagonal, rows grp + 16 meet 31 - L
+  cplx qu0 = cmake(grp == L ? 1.0 : 0.0, 0.0), qu1 = cmake(0.0, 0.0);
+  cplx ql0 = cmake(0.0, 0.0), ql1 = cmake(grp + 16 == JC - 1 - L ? 1.0 : 0.0, 0.0);
   for (int step = 0; step < JC - 1; ++step) {
-    auto idx = [&](int pos) { return pos == 0 ? 0 : 1 + (pos - 1 + step) % (JC - 1); };
-    auto pq = [&](int P, int& p, int& q) {
-      p = idx(P);
-      q = idx(JC - 1 - P);
-      if (p > q) { int tmp = p; p = q; q = tmp; }
-    };
-    // ---- phase A: rotations (zero-division form) and operand loads
-    if (tid < JC / 2) {
+    // ---- phase A: rotations (zero-division form) and block operands
+    if (rt >= 0 && rt < JC / 2) {
       int p, q;
-      pq(tid, p, q);
-      const double a = S.G[p][p].x, d = S.G[q][q].x;
-      const double2 g = S.G[p][q];
+      inner_pq(rt, step, p, q);
+      const double a = S.u.G[p][p].x, d = S.u.G[q][q].x;
+      const double2 g = S.u.G[p][q];
       const double g2 = g.x * g.x + g.y * g.y;
       double c = 1.0;
       double2 se = make_double2(0.0, 0.0);
@@ -277,162 +305,162 @@ __global__ __launch_bounds__(JNT) void jacobi_gram_kernel(const SectorDesc* __re
         const double f = copysign(ir * ic, dd);
         se = make_double2(f * g.x, f * g.y);
       }
-      S.rc[tid] = c;
-      S.rs[tid] = se;
+      S.rc[rt] = c;
+      S.rs[rt] = se;
     }
-    int p1 = 0, q1 = 0, p2 = 0, q2 = 0, pa, qa;
-    double2 b00 = make_double2(0, 0), b01 = b00, b10 = b00, b11 = b00;
+    int p1 = 0, q1 = 0, p2 = 0, q2 = 0;
+    cplx B00 = cmake(0.0, 0.0), B01 = B00, B10 = B00, B11 = B00;
     if (P1 >= 0) {
-      pq(P1, p1, q1);
-      pq(P2, p2, q2);
-      b00 = S.G[p1][p2]; b01 = S.G[p1][q2]; b10 = S.G[q1][p2]; b11 = S.G[q1][q2];
+      inner_pq(P1, step, p1, q1);
+      inner_pq(P2, step, p2, q2);
+      B00 = gget(S, p1, p2);
+      B01 = gget(S, p1, q2);
+      B10 = gget(S, q1, p2);
+      B11 = gget(S, q1, q2);
     }
-    pq(qp, pa, qa);
-    const double2 qv0 = S.Q[qr][pa], qw0 = S.Q[qr][qa];
-    const double2 qv1 = S.Q[qr + 16][pa], qw1 = S.Q[qr + 16][qa];
+    const int cu = circle_at(L, step, JC), cl = circle_at(JC - 1 - L, step, JC);
     __syncthreads();
-    // ---- phase B: updates
+    // ---- phase B: block updates G' = J^H G J, and Q' = Q J
     if (P1 >= 0) {
       const double c1 = S.rc[P1], c2v = S.rc[P2];
       const cplx s1 = cmake(S.rs[P1].x, S.rs[P1].y), s2 = cmake(S.rs[P2].x, S.rs[P2].y);
       const bool r1 = !(c1 == 1.0 && s1.x == 0.0 && s1.y == 0.0);
       const bool r2 = !(c2v == 1.0 && s2.x == 0.0 && s2.y == 0.0);
       if (r1 || r2) {
-        const cplx B00 = cmake(b00.x, b00.y), B01 = cmake(b01.x, b01.y);
-        const cplx B10 = cmake(b10.x, b10.y), B11 = cmake(b11.x, b11.y);
         // B J2: columns (p2, q2)
         const cplx x00 = csub(cscale(B00, c2v), cmulc(B01, s2)), x01 = cadd(cmul(B00, s2), cscale(B01, c2v));
         const cplx x10 = csub(cscale(B10, c2v), cmulc(B11, s2)), x11 = cadd(cmul(B10, s2), cscale(B11, c2v));
         // J1^H (B J2): rows (p1, q1)
-        cplx y00 = csub(cscale(x00, c1), cmul(s1, x10)), y01 = csub(cscale(x01, c1), cmul(s1, x11));
-        cplx y10 = cadd(cmulc(x00, s1), cscale(x10, c1)), y11 = cadd(cmulc(x01, s1), cscale(x11, c1));
+        const cplx y00 = csub(cscale(x00, c1), cmul(s1, x10)), y01 = csub(cscale(x01, c1), cmul(s1, x11));
+        const cplx y10 = cadd(cmulc(x00, s1), cscale(x10, c1)), y11 = cadd(cmulc(x01, s1), cscale(x11, c1));
         if (P1 == P2) {
-          y01 = cmake(0.0, 0.0);
-          y10 = cmake(0.0, 0.0);
-          y00.y = 0.0;
-          y11.y = 0.0;
-          S.G[p1][p1] = make_double2(y00.x, y00.y);
-          S.G[p1][q1] = make_double2(y01.x, y01.y);
-          S.G[q1][p1] = make_double2(y10.x, y10.y);
-          S.G[q1][q1] = make_double2(y11.x, y11.y);
+          S.u.G[p1][p1] = make_double2(y00.x, 0.0);
+          S.u.G[p1][q1] = make_double2(0.0, 0.0);
+          S.u.G[q1][q1] = make_double2(y11.x, 0.0);
         } else {
-          S.G[p1][p2] = make_double2(y00.x, y00.y);
-          S.G[p1][q2] = make_double2(y01.x, y01.y);
-          S.G[q1][p2] = make_double2(y10.x, y10.y);
-          S.G[q1][q2] = make_double2(y11.x, y11.y);
-          // Hermitian mirror
-          S.G[p2][p1] = make_double2(y00.x, -y00.y);
-          S.G[q2][p1] = make_double2(y01.x, -y01.y);
-          S.G[p2][q1] = make_double2(y10.x, -y10.y);
-          S.G[q2][q1] = make_double2(y11.x, -y11.y);
+          gput(S, p1, p2, y00);
+          gput(S, p1, q2, y01);
+          gput(S, q1, p2, y10);
+          gput(S, q1, q2, y11);
         }
       }
     }
     {
-      const double c = S.rc[qp];
-      const cplx se = cmake(S.rs[qp].x, S.rs[qp].y);
+      const double c = S.rc[L];
+      const cplx se = cmake(S.rs[L].x, S.rs[L].y);
       if (!(c == 1.0 && se.x == 0.0 && se.y == 0.0)) {
-        const cplx v0 = cmake(qv0.x, qv0.y), w0 = cmake(qw0.x, qw0.y);
-        const cplx v1 = cmake(qv1.x, qv1.y), w1 = cmake(qw1.x, qw1.y);
+        // columns (p, q) = (cu, cl) or (cl, cu): v = Q[:, p], w = Q[:, q]
+        const bool up = cu < cl;
+        const cplx v0 = up ? qu0 : ql0, w0 = up ? ql0 : qu0;
+        const cplx v1 = up ? qu1 : ql1, w1 = up ? ql1 : qu1;
         const cplx n0 = csub(cscale(v0, c), cmulc(w0, se)), m0 = cadd(cmul(v0, se), cscale(w0, c));
         const cplx n1 = csub(cscale(v1, c), cmulc(w1, se)), m1 = cadd(cmul(v1, se), cscale(w1, c));
-        S.Q[qr][pa] = make_double2(n0.x, n0.y);
-        S.Q[qr][qa] = make_double2(m0.x, m0.y);
-        S.Q[qr + 16][pa] = make_double2(n1.x, n1.y);
-        S.Q[qr + 16][qa] = make_double2(m1.x, m1.y);
+        qu0 = up ? n0 : m0;
+        ql0 = up ? m0 : n0;
+        qu1 = up ? n1 : m1;
+        ql1 = up ? m1 : n1;
       }
+      // turn the circle: position j takes the column of position j + 1 (31 -> 1), so
+      // pair L's upper entry comes from pair L + 1's upper (pair 15: its own lower) and
+      // its lower from pair L - 1's lower (pair 0: pair 1's upper); position 0 stays
+      const cplx du0 = cmake(__shfl_down_sync(0xffffffffu, qu0.x, 1, 16), __shfl_down_sync(0xffffffffu, qu0.y, 1, 16));
+      const cplx du1 = cmake(__shfl_down_sync(0xffffffffu, qu1.x, 1, 16), __shfl_down_sync(0xffffffffu, qu1.y, 1, 16));
+      const cplx ul0 = cmake(__shfl_up_sync(0xffffffffu, ql0.x, 1, 16), __shfl_up_sync(0xffffffffu, ql0.y, 1, 16));
+      const cplx ul1 = cmake(__shfl_up_sync(0xffffffffu, ql1.x, 1, 16), __shfl_up_sync(0xffffffffu, ql1.y, 1, 16));
+      const cplx nu0 = L == 0 ? qu0 : (L == 15 ? ql0 : du0), nu1 = L == 0 ? qu1 : (L == 15 ? ql1 : du1);
+      const cplx nl0 = L == 0 ? du0 : ul0, nl1 = L == 0 ? du1 : ul1;
+      qu0 = nu0;
+      qu1 = nu1;
+      ql0 = nl0;
+      ql1 = nl1;
     }
     __syncthreads();
   }
-  // ---- 6. Q and the flag for K2
-  cplx* qo = qbuf + (int64_t)T.gslot * JC * JC;
-  for (int e = tid; e < JC * JC; e += JNT) {
-    const double2 v = S.Q[e / JC][e % JC];
-    qo[e] = cmake(v.x, v.y);
-  }
-  if (tid == 0) qflag[T.gslot] = 1;
+  // ---- Q (column order again) and the flag for the apply kernel
+  cplx* qo = qbuf + (int64_t)T.slot * JC * JC;
+  stc(qo + grp * JC + L, qu0);
+  stc(qo + (grp + 16) * JC + L, qu1);
+  stc(qo + grp * JC + (JC - 1 - L), ql0);
+  stc(qo + (grp + 16) * JC + (JC - 1 - L), ql1);
+  if (tid == 0) qflag[T.slot] = 1;
 }
 
-// K2 of a round: every CTA of a rotated pair applies Q to its rows on the FP64 tensor
-// path: warp w owns rows [16 w, 16 w + 16) (two 8-row tiles) x the four 8-column tiles;
+// Round kernel 2: every part of a rotated pair applies Q to its rows on the FP64 tensor
+// path, straight from global memory into mma fragments: warp w owns rows
+// [16 w, 16 w + 16) (two 8-row tiles) x the four 8-column tiles;
 // (tr + i ti)(qr + i qi) = (tr qr - ti qi) + i (tr qi + ti qr)
-struct ApplySmem {
-  double2 tile[RMAX][JC + 1];
-  double2 Q[JC][JC + 1];
-  int cols[JC];
-};
-
 __global__ __launch_bounds__(JNT) void jacobi_apply_kernel(const SectorDesc* __restrict__ sd,
                                                            const JacobiWork* __restrict__ work,
                                                            int n_work, int t, cplx* __restrict__ abuf,
                                                            int max_sweeps,
                                                            const cplx* __restrict__ qbuf,
                                                            const int* __restrict__ qflag) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  ApplySmem& S = *reinterpret_cast<ApplySmem*>(smem_raw);
+  __shared__ double2 Qs[JC][JC + 1];
+  __shared__ int cols[JC];
   const int tid = threadIdx.x;
-  const JacTask T = jac_task(work, n_work, t);
-  if (!T.valid || T.sweep >= max_sweeps) return;
-  if (!qflag[T.gslot]) return;   // converged sector, or a pair without rotation
+  const JacTask T = jac_task(work, n_work, t, true);
+  if (T.sweep >= max_sweeps) return;
+  if (!qflag[T.slot]) return;   // converged sector, or a pair without rotation
   const SectorDesc& D = sd[T.W.sector];
   const int k = D.k;
-  int r0, nr, ng;
-  jac_rows(T, D.rows_tot, D.rows_g, r0, nr, ng);
-  if (nr == 0) return;
-  if (tid < JC) S.cols[tid] = jac_col(T, tid, k);
-  const cplx* qi = qbuf + (int64_t)T.gslot * JC * JC;
-  for (int e = tid; e < JC * JC; e += JNT) {
+  const int r0 = T.part * T.W.chunk;
+  const int nr = min(D.rows_tot, r0 + T.W.chunk) - r0;
+  if (tid < JC) cols[tid] = jac_col(T, tid, k);
+  const cplx* qi = qbuf + (int64_t)T.slot * JC * JC;
+#pragma unroll
+  for (int i = 0; i < JC * JC / JNT; ++i) {
+    const int e = tid + i * JNT;
     const cplx v = ldc(qi + e);
-    S.Q[e / JC][e % JC] = make_double2(v.x, v.y);
+    Qs[e / JC][e % JC] = make_double2(v.x, v.y);
   }
   __syncthreads();
   cplx* A = abuf + D.a_off;
-  for (int e = tid; e < nr * JC; e += JNT) {
-    const int r = e / JC, c = e % JC;
-    double2 v = make_double2(0.0, 0.0);
-    if (S.cols[c] >= 0) v = *reinterpret_cast<const double2*>(A + (int64_t)(r0 + r) * k + S.cols[c]);
-    S.tile[r][c] = v;
-  }
-  __syncthreads();
   const int warp = tid >> 5, lane = tid & 31, li = lane >> 2, lk = lane & 3;
-  if (16 * warp < nr) {
-    double2 ore[2][4], oim[2][4];
+  if (16 * warp >= nr) return;
+  double2 tv[2][JC / 4];
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+    const int row = 16 * warp + 8 * a + li;
+#pragma unroll
+    for (int kk = 0; kk < JC / 4; ++kk) {
+      const int col = cols[4 * kk + lk];
+      tv[a][kk] = make_double2(0.0, 0.0);
+      if (row < nr && col >= 0) tv[a][kk] = *reinterpret_cast<const double2*>(A + (int64_t)(r0 + row) * k + col);
+    }
+  }
+  double2 ore[2][4], oim[2][4];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) { ore[a][c] = make_double2(0, 0); oim[a][c] = make_double2(0, 0); }
+#pragma unroll
+  for (int kk = 0; kk < JC / 4; ++kk) {
+    double2 q[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) q[c] = Qs[4 * kk + lk][8 * c + li];
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) { ore[a][c] = make_double2(0, 0); oim[a][c] = make_double2(0, 0); }
-#pragma unroll
-    for (int k0 = 0; k0 < JC; k0 += 4) {
-      double2 tv[2], q[4];
-#pragma unroll
-      for (int a = 0; a < 2; ++a) tv[a] = S.tile[16 * warp + 8 * a + li][k0 + lk];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) q[c] = S.Q[k0 + lk][8 * c + li];
-#pragma unroll
-      for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          dmma(ore[a][c], tv[a].x, q[c].x);
-          dmma(ore[a][c], -tv[a].y, q[c].y);
-          dmma(oim[a][c], tv[a].x, q[c].y);
-          dmma(oim[a][c], tv[a].y, q[c].x);
-        }
-    }
-#pragma unroll
-    for (int a = 0; a < 2; ++a) {
-      const int row = 16 * warp + 8 * a + li;
-      if (row >= nr) continue;
-#pragma unroll
       for (int c = 0; c < 4; ++c) {
-        const int c0 = S.cols[8 * c + 2 * lk], c1 = S.cols[8 * c + 2 * lk + 1];
-        if (c0 >= 0) stc(A + (int64_t)(r0 + row) * k + c0, cmake(ore[a][c].x, oim[a][c].x));
-        if (c1 >= 0) stc(A + (int64_t)(r0 + row) * k + c1, cmake(ore[a][c].y, oim[a][c].y));
+        dmma(ore[a][c], tv[a][kk].x, q[c].x);
+        dmma(ore[a][c], -tv[a][kk].y, q[c].y);
+        dmma(oim[a][c], tv[a][kk].x, q[c].y);
+        dmma(oim[a][c], tv[a][kk].y, q[c].x);
       }
+  }
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+    const int row = 16 * warp + 8 * a + li;
+    if (row >= nr) continue;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int c0 = cols[8 * c + 2 * lk], c1 = cols[8 * c + 2 * lk + 1];
+      if (c0 >= 0) stc(A + (int64_t)(r0 + row) * k + c0, cmake(ore[a][c].x, oim[a][c].x));
+      if (c1 >= 0) stc(A + (int64_t)(r0 + row) * k + c1, cmake(ore[a][c].y, oim[a][c].y));
     }
   }
 }
 
-// column norms + descending sort (ties by column index), one CTA per sector
 constexpr int FNT = 512;
 
 __global__ __launch_bounds__(FNT) void jacobi_finish_kernel(const SectorDesc* __restrict__ sd,
@@ -520,49 +548,30 @@ cudaError_t launch_sector_norms(const SectorDesc* sd_dev, int n_sectors, const v
 }
 
 cudaError_t launch_jacobi_round(const SectorDesc* sd_dev, const JacobiWork* work_dev, int n_work,
-                                int total_clusters, int t, void* abuf, int* rot_count,
-                                const double* nf2, double tol, int max_sweeps, void* qbuf,
-                                int* qflag, cudaStream_t s) {
-  if (total_clusters <= 0) return cudaSuccess;
+                                int gram_ctas, int apply_ctas, int t, void* abuf, int* rot_count,
+                                const double* nf2, double tol, int max_sweeps, void* pbuf,
+                                int* pcnt, void* qbuf, int* qflag, cudaStream_t s) {
+  if (gram_ctas <= 0) return cudaSuccess;
   static bool attr_done = false;
-  const int smem1 = (int)sizeof(JacSmem), smem2 = (int)sizeof(ApplySmem);
+  const int smem1 = (int)sizeof(GramSmem);
   if (!attr_done) {
     cudaError_t e = cudaFuncSetAttribute(jacobi_gram_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem1);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(jacobi_gram_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(jacobi_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2);
     if (e != cudaSuccess) return e;
     attr_done = true;
   }
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(total_clusters * JCL, 1, 1);
-  cfg.blockDim = dim3(JNT, 1, 1);
-  cfg.dynamicSmemBytes = smem1;
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = JCL;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  cudaError_t e = cudaLaunchKernelEx(&cfg, jacobi_gram_kernel, sd_dev, work_dev, n_work, t,
-                                     reinterpret_cast<const cplx*>(abuf), rot_count, nf2, tol,
-                                     max_sweeps, reinterpret_cast<cplx*>(qbuf), qflag);
+  jacobi_gram_kernel<<<gram_ctas, JNT, smem1, s>>>(
+      sd_dev, work_dev, n_work, t, reinterpret_cast<const cplx*>(abuf), rot_count, nf2, tol,
+      max_sweeps, reinterpret_cast<cplx*>(pbuf), pcnt, reinterpret_cast<cplx*>(qbuf), qflag);
+  cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  jacobi_apply_kernel<<<total_clusters * JCL, JNT, smem2, s>>>(
-      sd_dev, work_dev, n_work, t, reinterpret_cast<cplx*>(abuf), max_sweeps,
-      reinterpret_cast<const cplx*>(qbuf), qflag);
+  jacobi_apply_kernel<<<apply_ctas, JNT, 0, s>>>(sd_dev, work_dev, n_work, t,
+                                                 reinterpret_cast<cplx*>(abuf), max_sweeps,
+                                                 reinterpret_cast<const cplx*>(qbuf), qflag);
   return cudaGetLastError();
 }
 
-int jacobi_qslots(int total_clusters) { return total_clusters * JCL; }
-
-int jacobi_max_rows() { return JCL * RMAX; }
-int jacobi_cluster_ctas() { return JCL; }
-int jacobi_rows_per_cta() { return RMAX; }
+int jacobi_rows_per_part() { return RMAX; }
 
 cudaError_t launch_jacobi_finish(const SectorDesc* sd_dev, int n_sectors, int max_k,
                                  const void* abuf, const double* nf2, double* sig, int* perm,

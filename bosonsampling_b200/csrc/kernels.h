@@ -127,25 +127,26 @@ struct JacobiWork {
   int nblk;         // column blocks
   int npairs;       // block pairs per round
   int rounds;       // rounds per sweep
-  int cta_start;    // first cluster index of this sector
-  int cs;           // CTAs per block pair (rows split cs ways); a cluster holds 8/cs pairs
-  int clusters;     // clusters of this sector
-  int pad_;
+  int cs;           // row parts per block pair (rows_tot in parts of `chunk` rows)
+  int cs_g;         // parts holding Gram rows (the first rows_g rows)
+  int chunk;        // rows per part (multiple of 16, at most jacobi_rows_per_part())
+  int gram_start;   // first CTA of this sector in the gram launch (npairs * cs_g CTAs)
+  int apply_start;  // first CTA in the apply launch (npairs * cs CTAs)
+  int slot_start;   // first block-pair slot (Q, flag and arrival counter)
+  int pad_[2];
 };
-// CTAs per cluster and rows a CTA holds in shared memory
-int jacobi_cluster_ctas();
-int jacobi_rows_per_cta();
+// rows of one part of a block pair
+int jacobi_rows_per_part();
 int jacobi_block_cols();
-// Two launches: the pair Gram + test + inner Jacobi sweep (clusters), then the rotation
-// of every pair's rows.  qbuf holds jacobi_qslots(total_clusters) 32 x 32 complex
-// rotations, qflag as many ints.
+// One round of every listed sector: the gram kernel (partial Grams -> pbuf, 32 x 32
+// complex per gram CTA; the last part of a pair reduces, tests and solves, writing Q
+// and the flag of its slot), then the apply kernel.  pcnt (one int per slot) must be
+// zero before the first round; the kernels leave it zero.
 cudaError_t launch_jacobi_round(const SectorDesc* sd_dev, const JacobiWork* work_dev, int n_work,
-                                int total_clusters, int t, void* abuf, int* rot_count,
-                                const double* nf2, double tol, int max_sweeps, void* qbuf,
-                                int* qflag, cudaStream_t s);
-int jacobi_qslots(int total_clusters);
+                                int gram_ctas, int apply_ctas, int t, void* abuf, int* rot_count,
+                                const double* nf2, double tol, int max_sweeps, void* pbuf,
+                                int* pcnt, void* qbuf, int* qflag, cudaStream_t s);
 // Largest number of Jacobi-matrix rows (|L| + |R| or |L|) a sector may have.
-int jacobi_max_rows();
 // ||T_s||_F^2 of each sector's Jacobi matrix (Gram rows), fixed-order reduction.
 cudaError_t launch_sector_norms(const SectorDesc* sd_dev, int n_sectors, const void* abuf,
                                 double* nf2, cudaStream_t s);
