@@ -759,7 +759,7 @@ int bsmpo_destroy(bsmpo_ctx* h) {
   DevBuf* bufs[] = {&h->theta, &h->cbuf, &h->abuf, &h->wbuf, &h->vbuf, &h->sig, &h->keys,
                     &h->perm, &h->tab, &h->tab2, &h->rot, &h->kept, &h->u3, &h->m4,
                     &h->env_l, &h->env_r, &h->part, &h->outv, &h->dims, &h->nf2, &h->qbuf,
-                    &h->qflag};
+                    &h->qflag, &h->pbuf, &h->pcnt};
   for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
   HostStage* hs[] = {&h->stage, &h->stage2, &h->hres};
   for (HostStage* b : hs) if (b->p) cudaFreeHost(b->p);
