@@ -50,6 +50,9 @@ def parse():
     p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work per sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="chi1024", choices=sorted(WORKLOADS))
+    p.add_argument("--bs-per-step", type=int, default=0,
+                   help="profiling runs only: a step runs the first N beam splitters of its layer "
+                        "(0: the whole layer)")
     p.add_argument("--state-cache", default=None,
                    help="file holding the state at --start-layer: loaded if present (the untimed "
                         "set-up layers are skipped), else written after them; for profiling runs, "
@@ -223,8 +226,8 @@ def main():
     sim = engine.MPOSimulator(w["n"], w["d"], w["chi"])
     sim.init_single_photons(range(0, w["n"], 2), w["eta"])
 
-    def run_layer(L):
-        ops = layers[L]
+    def run_layer(L, partial=False):
+        ops = layers[L][:args.bs_per_step] if (partial and args.bs_per_step > 0) else layers[L]
         sim.run_mesh([m for (m, _, _) in ops], [t for (_, t, _) in ops], [p for (_, _, p) in ops])
 
     # untimed: advance to the saturated middle of the circuit
@@ -258,6 +261,8 @@ def main():
     # ---- timed, device-resident: K layers after the warm-up ones
     first = args.start_layer + args.warmup
     n_bs = sum(len(layers[first + i]) for i in range(args.steps))
+    if args.bs_per_step > 0:
+        n_bs = sum(min(args.bs_per_step, len(layers[first + i])) for i in range(args.steps))
     sampler = ClockSampler(local)
     sim.set_timing(True)
     launches0 = sim.kernel_launches()
@@ -269,7 +274,7 @@ def main():
     torch.cuda.nvtx.range_push("timed")
     e0.record()
     for i in range(args.steps):
-        run_layer(first + i)
+        run_layer(first + i, partial=True)
     e1.record()
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
@@ -342,6 +347,7 @@ def main():
                        "circuit_time_s_upper_est": round(len(bs) / (value / world), 1),
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (state %.2f GB)" % (g_host.numel() * 16 / 1e9),
+                       "bs_per_step": args.bs_per_step or "whole layer",
                        "cutoff": 0.0},
             "e2e": {"value": world * n_bs_e2e / t_e2e, "unit": "BS-updates/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},

@@ -32,14 +32,6 @@ __device__ __forceinline__ void dmma(double2& d, double a, double b) {
                : "d"(a), "d"(b));
 }
 
-// Programmatic dependent launch: the round kernels let the next kernel of the stream
-// start launching at once (its CTAs then wait for this grid in pdl_wait), hiding the
-// launch latency between the rounds' kernels.
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-// Blocks until the previous kernel of the stream has completed and its writes are visible
-// (returns at once when this grid was launched without the dependency attribute).
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-
 constexpr int JB = 16;        // columns per block
 constexpr int JC = 2 * JB;    // columns per block pair
 constexpr int JNT = 256;
@@ -152,7 +144,6 @@ __global__ __launch_bounds__(JNT) void jacobi_gram_kernel(const SectorDesc* __re
   extern __shared__ __align__(16) unsigned char smem_raw[];
   GramSmem& S = *reinterpret_cast<GramSmem*>(smem_raw);
   const int tid = threadIdx.x;
-  pdl_wait();
   const JacTask T = jac_task(work, n_work, t, false);
   if (T.part == 0 && tid == 0) qflag[T.slot] = 0;
   // every exit before the arrival counter depends on (sector, t) only
@@ -274,7 +265,6 @@ __global__ __launch_bounds__(JNT) void jacobi_gram_kernel(const SectorDesc* __re
   __syncthreads();
   if (!S.rotate) return;
   if (tid == 0) atomicAdd(cnt + T.sweep % 3, 1);
-  pdl_trigger();   // the apply kernel may launch during the sweep (other CTAs: at exit)
 
   // ---- c. one cyclic Jacobi sweep on the Gram
   // block roles: thread < 136 updates the 2 x 2 block (P1, P2), P1 <= P2, of the pair
@@ -408,7 +398,6 @@ __global__ __launch_bounds__(JNT) void jacobi_apply_kernel(const SectorDesc* __r
   __shared__ double2 Qs[JC][JC + 1];
   __shared__ int cols[JC];
   const int tid = threadIdx.x;
-  pdl_wait();
   const JacTask T = jac_task(work, n_work, t, true);
   if (T.sweep >= max_sweeps) return;
   if (!qflag[T.slot]) return;   // converged sector, or a pair without rotation
@@ -568,39 +557,17 @@ cudaError_t launch_jacobi_round(const SectorDesc* sd_dev, const JacobiWork* work
   if (!attr_done) {
     cudaError_t e = cudaFuncSetAttribute(jacobi_gram_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem1);
-    // both round kernels on the largest shared-memory carveout: no L1/shared
-    // reconfiguration of an SM between them
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(jacobi_gram_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                               (int)cudaSharedmemCarveoutMaxShared);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(jacobi_apply_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                               (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     attr_done = true;
   }
-  cudaLaunchAttribute pdl[1];
-  pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  pdl[0].val.programmaticStreamSerializationAllowed = 1;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(gram_ctas, 1, 1);
-  cfg.blockDim = dim3(JNT, 1, 1);
-  cfg.dynamicSmemBytes = smem1;
-  cfg.stream = s;
-  cfg.attrs = pdl;
-  cfg.numAttrs = 0;   // the gram kernel waits for the previous round in full
-  cudaError_t e = cudaLaunchKernelEx(&cfg, jacobi_gram_kernel, sd_dev, work_dev, n_work, t,
-                                     reinterpret_cast<const cplx*>(abuf), rot_count, nf2, tol,
-                                     max_sweeps, reinterpret_cast<cplx*>(pbuf), pcnt,
-                                     reinterpret_cast<cplx*>(qbuf), qflag);
+  jacobi_gram_kernel<<<gram_ctas, JNT, smem1, s>>>(
+      sd_dev, work_dev, n_work, t, reinterpret_cast<const cplx*>(abuf), rot_count, nf2, tol,
+      max_sweeps, reinterpret_cast<cplx*>(pbuf), pcnt, reinterpret_cast<cplx*>(qbuf), qflag);
+  cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  cfg.gridDim = dim3(apply_ctas, 1, 1);
-  cfg.dynamicSmemBytes = 0;
-  cfg.numAttrs = 1;
-  e = cudaLaunchKernelEx(&cfg, jacobi_apply_kernel, sd_dev, work_dev, n_work, t,
-                         reinterpret_cast<cplx*>(abuf), max_sweeps,
-                         reinterpret_cast<const cplx*>(qbuf), static_cast<const int*>(qflag));
-  if (e != cudaSuccess) return e;
+  jacobi_apply_kernel<<<apply_ctas, JNT, 0, s>>>(sd_dev, work_dev, n_work, t,
+                                                 reinterpret_cast<cplx*>(abuf), max_sweeps,
+                                                 reinterpret_cast<const cplx*>(qbuf), qflag);
   return cudaGetLastError();
 }
 
