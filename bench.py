@@ -50,9 +50,9 @@ def parse():
     p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work per sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="chi1024", choices=sorted(WORKLOADS))
-    p.add_argument("--bs-per-step", type=int, default=0,
-                   help="profiling runs only: a step runs the first N beam splitters of its layer "
-                        "(0: the whole layer)")
+    p.add_argument("--bs-slice", default=None,
+                   help="profiling runs only: START:STOP -- a step runs beam splitters START..STOP-1 "
+                        "of its layer (default: the whole layer)")
     p.add_argument("--state-cache", default=None,
                    help="file holding the state at --start-layer: loaded if present (the untimed "
                         "set-up layers are skipped), else written after them; for profiling runs, "
@@ -226,8 +226,10 @@ def main():
     sim = engine.MPOSimulator(w["n"], w["d"], w["chi"])
     sim.init_single_photons(range(0, w["n"], 2), w["eta"])
 
+    bs_slice = slice(*[int(x) for x in args.bs_slice.split(":")]) if args.bs_slice else slice(None)
+
     def run_layer(L, partial=False):
-        ops = layers[L][:args.bs_per_step] if (partial and args.bs_per_step > 0) else layers[L]
+        ops = layers[L][bs_slice] if partial else layers[L]
         sim.run_mesh([m for (m, _, _) in ops], [t for (_, t, _) in ops], [p for (_, _, p) in ops])
 
     # untimed: advance to the saturated middle of the circuit
@@ -260,9 +262,7 @@ def main():
 
     # ---- timed, device-resident: K layers after the warm-up ones
     first = args.start_layer + args.warmup
-    n_bs = sum(len(layers[first + i]) for i in range(args.steps))
-    if args.bs_per_step > 0:
-        n_bs = sum(min(args.bs_per_step, len(layers[first + i])) for i in range(args.steps))
+    n_bs = sum(len(layers[first + i][bs_slice]) for i in range(args.steps))
     sampler = ClockSampler(local)
     sim.set_timing(True)
     launches0 = sim.kernel_launches()
@@ -347,7 +347,7 @@ def main():
                        "circuit_time_s_upper_est": round(len(bs) / (value / world), 1),
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (state %.2f GB)" % (g_host.numel() * 16 / 1e9),
-                       "bs_per_step": args.bs_per_step or "whole layer",
+                       "bs_slice": args.bs_slice or "whole layer",
                        "cutoff": 0.0},
             "e2e": {"value": world * n_bs_e2e / t_e2e, "unit": "BS-updates/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
@@ -358,7 +358,11 @@ def main():
                          "peak_source": "FP64 DGEMM measured in this run (torch.matmul 8192^3, best of 5)",
                          "jacobi_device_ms": jac_ms, "jacobi_launches": jac_launches,
                          "jacobi_share_of_step": (jac_ms / 1e3) / t_dev if t_dev else None,
-                         "traffic": None},
+                         # DRAM bytes (read + write) of one early-round jacobi_gram_kernel
+                         # launch of this workload under ncu (cold cache; see
+                         # profiles/jacobi_round_kernels_chi1024.md)
+                         "traffic": 21995008 if args.workload == "chi1024" else None,
+                         "traffic_unit": "bytes per launch"},
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
