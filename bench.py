@@ -359,8 +359,7 @@ def main():
                          "jacobi_device_ms": jac_ms, "jacobi_launches": jac_launches,
                          "jacobi_share_of_step": (jac_ms / 1e3) / t_dev if t_dev else None,
                          # DRAM bytes (read + write) of one early-round jacobi_gram_kernel
-                         # launch of this workload under ncu (cold cache; see
-                         # profiles/jacobi_round_kernels_chi1024.md)
+                         # launch of this workload, measured with ncu (cold cache)
                          "traffic": 21995008 if args.workload == "chi1024" else None,
                          "traffic_unit": "bytes per launch"},
             "clocks": clocks,
