@@ -187,18 +187,31 @@ __global__ __launch_bounds__(JNT) void jacobi_gram_kernel(const SectorDesc* __re
   }
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31, li = lane >> 2, lk = lane & 3;
-  // G[i][j] = sum_r conj(X[r][i]) X[r][j]: warp w owns the 8 x 8 tiles (I, J) =
-  // (w / 2, 2 (w % 2) + {0, 1}); rows in chunks of 4;
+  // G[i][j] = sum_r conj(X[r][i]) X[r][j] on 8 x 8 tiles, rows in chunks of 4;
   // (ar - i ai)(br + i bi) = (ar br + ai bi) + i (ar bi - ai br)
-  const int I = warp >> 1, J0 = 2 * (warp & 1);
+  // The Gram is Hermitian: only its 10 upper 8 x 8 tiles (I <= J) are formed, spread
+  // over the warps so that no scheduler (warps w and w + 4) carries more than three.
+  int I0, J0, I1 = 0, J1 = 0, nt = 1;
+  switch (warp) {
+    case 0: I0 = 0; J0 = 0; I1 = 0; J1 = 1; nt = 2; break;
+    case 1: I0 = 0; J0 = 3; I1 = 1; J1 = 1; nt = 2; break;
+    case 2: I0 = 1; J0 = 3; break;
+    case 3: I0 = 2; J0 = 3; break;
+    case 4: I0 = 0; J0 = 2; break;
+    case 5: I0 = 1; J0 = 2; break;
+    case 6: I0 = 2; J0 = 2; break;
+    default: I0 = 3; J0 = 3; break;
+  }
   double2 gre[2] = {make_double2(0, 0), make_double2(0, 0)};
   double2 gim[2] = {make_double2(0, 0), make_double2(0, 0)};
   for (int k0 = 0; k0 < ng; k0 += 4) {
     const int r = k0 + lk;
-    const double2 a = r < ng ? S.u.tile[r][8 * I + li] : make_double2(0.0, 0.0);
 #pragma unroll
     for (int jj = 0; jj < 2; ++jj) {
-      const double2 b = r < ng ? S.u.tile[r][8 * (J0 + jj) + li] : make_double2(0.0, 0.0);
+      if (jj >= nt) break;   // warp-uniform
+      const int I = jj == 0 ? I0 : I1, J = jj == 0 ? J0 : J1;
+      const double2 a = r < ng ? S.u.tile[r][8 * I + li] : make_double2(0.0, 0.0);
+      const double2 b = r < ng ? S.u.tile[r][8 * J + li] : make_double2(0.0, 0.0);
       dmma(gre[jj], a.x, b.x);
       dmma(gre[jj], a.y, b.y);
       dmma(gim[jj], a.x, b.y);
@@ -210,7 +223,8 @@ __global__ __launch_bounds__(JNT) void jacobi_gram_kernel(const SectorDesc* __re
   if (cs_g == 1) {
 #pragma unroll
     for (int jj = 0; jj < 2; ++jj) {
-      const int row = 8 * I + li, c0 = 8 * (J0 + jj) + 2 * lk;
+      if (jj >= nt) break;
+      const int row = 8 * (jj == 0 ? I0 : I1) + li, c0 = 8 * (jj == 0 ? J0 : J1) + 2 * lk;
       S.u.G[row][c0] = make_double2(gre[jj].x, gim[jj].x);
       S.u.G[row][c0 + 1] = make_double2(gre[jj].y, gim[jj].y);
     }
@@ -218,7 +232,8 @@ __global__ __launch_bounds__(JNT) void jacobi_gram_kernel(const SectorDesc* __re
     cplx* pp = pbuf + (int64_t)blockIdx.x * JC * JC;
 #pragma unroll
     for (int jj = 0; jj < 2; ++jj) {
-      const int row = 8 * I + li, c0 = 8 * (J0 + jj) + 2 * lk;
+      if (jj >= nt) break;
+      const int row = 8 * (jj == 0 ? I0 : I1) + li, c0 = 8 * (jj == 0 ? J0 : J1) + 2 * lk;
       __stcg(reinterpret_cast<double2*>(pp + row * JC + c0), make_double2(gre[jj].x, gim[jj].x));
       __stcg(reinterpret_cast<double2*>(pp + row * JC + c0 + 1), make_double2(gre[jj].y, gim[jj].y));
     }
