@@ -71,29 +71,61 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples while the timed region runs."""
+    """SM clock, power and clock-event (throttle) reasons while the timed region runs.
+
+    Reads them in-process through NVML every 0.5 s (a spawned nvidia-smi per sample
+    initialises NVML each time and competes with the timed process for the driver);
+    falls back to nvidia-smi when NVML is not importable.  Reads only."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
-        self.samples = []
+    def __init__(self, cuda_index, period=0.5):
+        self.cuda_index = cuda_index
+        self.period = period
+        self.samples = []   # (sm_mhz, sm_max_mhz, watts, set of reasons)
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+        self._h = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            pr = torch.cuda.get_device_properties(cuda_index)
+            bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            self._h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            self._nvml = pynvml
+        except Exception:
+            self._nvml = None
+
+    def _sample_nvml(self):
+        n, h = self._nvml, self._h
+        sm = n.nvmlDeviceGetClockInfo(h, n.NVML_CLOCK_SM)
+        mx = n.nvmlDeviceGetMaxClockInfo(h, n.NVML_CLOCK_SM)
+        w = n.nvmlDeviceGetPowerUsage(h) / 1e3
+        bits = n.nvmlDeviceGetCurrentClocksEventReasons(h)
+        return (float(sm), float(mx), w, {name for name, bit in self.REASONS if bits & bit})
+
+    def _sample_smi(self):
+        out = subprocess.run(["nvidia-smi", "-i", str(self.cuda_index), "--query-gpu=" + self.FIELDS,
+                              "--format=csv,noheader,nounits"], capture_output=True,
+                             text=True, timeout=5).stdout.strip()
+        f = [x.strip() for x in out.split(",")]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        return (float(f[1]), float(f[2]), float(f[3]) if f[3].replace(".", "").isdigit() else 0.0,
+                {nm for nm, v in zip(names, f[5:9]) if v.lower() == "active"})
 
     def _run(self):
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
-                                      "--format=csv,noheader,nounits"], capture_output=True,
-                                     text=True, timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([x.strip() for x in out.split(",")])
+                self.samples.append(self._sample_nvml() if self._nvml else self._sample_smi())
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(self.period)
 
     def start(self):
         self._t = threading.Thread(target=self._run, daemon=True)
@@ -107,17 +139,14 @@ class ClockSampler:
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
-        for s in self.samples:
-            for name, v in zip(names, s[5:9]):
-                if v.strip().lower() == "active":
-                    reasons.add(name)
-        return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+        for smp in self.samples:
+            reasons |= smp[3]
+        return {"sm_mhz": float(np.median([x[0] for x in self.samples])),
+                "sm_max_mhz": max(x[1] for x in self.samples),
+                "power_w_max": round(max(x[2] for x in self.samples), 1),
+                "reasons": sorted(reasons), "samples": len(self.samples),
+                "source": "nvml" if self._nvml else "nvidia-smi"}
 
 
 def layers_of(bs):
