@@ -11,6 +11,9 @@
 //   blocked one-sided Jacobi rounds -> column norms + sort -> top-chi selection ->
 //   [sync: kept counts] -> V extraction -> W = V^H C grouped GEMM -> scatter.
 #include <algorithm>
+#include <atomic>
+#include <mutex>
+#include <thread>
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
@@ -80,6 +83,15 @@ struct bsmpo_ctx {
   int last_ns = 0;
   int64_t launches = 0;
   std::string err;
+  // Concurrent updates of one brick-wall layer (bsmpo_run_mesh).  A worker context
+  // shares its owner's state and host mirror (cnt_shared) and owns its workspaces and
+  // stream; the owner keeps its workers and, after a mesh, points `diag` at the worker
+  // that ran the mesh's last update.
+  std::vector<int>* cnt_shared = nullptr;
+  std::vector<bsmpo_ctx*> workers;
+  int n_workers = 8;      // BSMPO_WORKERS / bsmpo_set_workers
+  const bsmpo_ctx* diag = nullptr;
+  int last_index = -1;    // worker: mesh index of the last update it ran
 };
 
 namespace {
@@ -89,6 +101,9 @@ int fail(bsmpo_ctx* h, int code, const std::string& msg) {
   g_last_error = msg;
   return code;
 }
+
+// the host mirror of the charge-block sizes (a worker's is its owner's)
+std::vector<int>& mirror(bsmpo_ctx* h) { return h->cnt_shared ? *h->cnt_shared : h->cnt; }
 
 #define CK(h, call)                                                                    \
   do {                                                                                 \
@@ -174,9 +189,10 @@ void jacobi_launch_list(std::vector<JacobiWork>& w, int* gram_ctas, int* apply_c
 
 int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
   const int d = h->d, dd = d * d;
-  const int* cL = &h->cnt[(size_t)mode * dd];
-  const int* cC = &h->cnt[(size_t)(mode + 1) * dd];
-  const int* cR = &h->cnt[(size_t)(mode + 2) * dd];
+  const std::vector<int>& cnt = mirror(h);
+  const int* cL = &cnt[(size_t)mode * dd];
+  const int* cC = &cnt[(size_t)(mode + 1) * dd];
+  const int* cR = &cnt[(size_t)(mode + 2) * dd];
   UpdateTables& T = P.tab;
   std::memset(&T, 0, sizeof(T));
   T.d = d;
@@ -601,15 +617,16 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   // algorithmic minimum bytes: read Glc, Gcr, write Gamma_L, Gamma_R (complex128)
   {
     double nl = 0, nc = 0, nr = 0;
+    const std::vector<int>& cnt = mirror(h);
     for (int q = 0; q < dd; ++q) {
-      nl += h->cnt[(size_t)mode * dd + q];
-      nc += h->cnt[(size_t)(mode + 1) * dd + q];
-      nr += h->cnt[(size_t)(mode + 2) * dd + q];
+      nl += cnt[(size_t)mode * dd + q];
+      nc += cnt[(size_t)(mode + 1) * dd + q];
+      nr += cnt[(size_t)(mode + 2) * dd + q];
     }
     h->last_bytes = 16.0 * (nl * nc + nc * nr + ((double)nl + nr) * total_kept);
   }
   // host mirror and diagnostics
-  int* cM = &h->cnt[(size_t)(mode + 1) * dd];
+  int* cM = &mirror(h)[(size_t)(mode + 1) * dd];
   std::fill(cM, cM + dd, 0);
   h->last_cc.assign(2 * ns, 0);
   h->last_shape.assign(2 * ns, 0);
@@ -645,6 +662,127 @@ M8 transpose_to_m8(const double* S) {
   m.v[4] = S[2]; m.v[5] = S[3];   // M10 = S01
   m.v[6] = S[6]; m.v[7] = S[7];   // M11 = S11
   return m;
+}
+
+void free_workspaces(bsmpo_ctx* h) {
+  DevBuf* bufs[] = {&h->theta, &h->cbuf, &h->abuf, &h->wbuf, &h->vbuf, &h->sig, &h->keys,
+                    &h->perm, &h->tab, &h->tab2, &h->rot, &h->kept, &h->u3, &h->m4,
+                    &h->env_l, &h->env_r, &h->part, &h->outv, &h->dims, &h->nf2, &h->qbuf,
+                    &h->qflag, &h->pbuf, &h->pcnt};
+  for (DevBuf* b : bufs)
+    if (b->p) cudaFree(b->p);
+  HostStage* hs[] = {&h->stage, &h->stage2, &h->hres};
+  for (HostStage* b : hs)
+    if (b->p) cudaFreeHost(b->p);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+}
+
+// A worker context for concurrent updates: the owner's state, its own stream.
+int make_worker(bsmpo_ctx* h, bsmpo_ctx** out) {
+  bsmpo_ctx* w = new bsmpo_ctx();
+  w->n = h->n; w->d = h->d; w->chi = h->chi; w->device = h->device;
+  w->gamma = h->gamma; w->lam = h->lam; w->charge = h->charge;
+  w->loaded = true;
+  w->cnt_shared = &h->cnt;
+  w->profile = h->profile;
+  if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete w;
+    return fail(h, BSMPO_ECUDA, "worker stream creation failed");
+  }
+  *out = w;
+  return BSMPO_OK;
+}
+
+void destroy_worker(bsmpo_ctx* w) {
+  cudaStreamSynchronize(w->stream);
+  free_workspaces(w);
+  cudaStreamDestroy(w->stream);
+  delete w;   // the state belongs to the owner
+}
+
+// Runs the updates of a mesh on the owner's workers: consecutive beam splitters whose
+// modes differ by 2 or more pairwise (one brick-wall layer) touch disjoint sites and
+// write disjoint bonds, so they run concurrently, one per worker stream; a layer ends
+// with every worker's stream drained (host barrier) before the next one starts.  Every
+// update computes exactly what it computes alone.
+int run_mesh_concurrent(bsmpo_ctx* h, int n_bs, const int* modes, const cplx* u3, int nw) {
+  const int d3 = h->d * h->d * h->d;
+  int rc;
+  while ((int)h->workers.size() < nw) {
+    bsmpo_ctx* w = nullptr;
+    if ((rc = make_worker(h, &w))) return rc;
+    h->workers.push_back(w);
+  }
+  for (int k = 0; k < nw; ++k) {
+    bsmpo_ctx* w = h->workers[k];
+    w->cutoff = h->cutoff;
+    w->jac_rows = h->jac_rows;
+    w->timing = h->timing;
+    if (w->timing && !w->ev0) {
+      CK(h, cudaEventCreate(&w->ev0));
+      CK(h, cudaEventCreate(&w->ev1));
+    }
+    w->last_index = -1;
+  }
+  std::mutex err_mutex;
+  int err_code = BSMPO_OK;
+  std::string err_msg;
+  for (int i = 0; i < n_bs;) {
+    int j = i + 1;
+    for (; j < n_bs; ++j) {
+      bool ok = true;
+      for (int l = i; l < j && ok; ++l) ok = std::abs(modes[j] - modes[l]) >= 2;
+      if (!ok) break;
+    }
+    std::atomic<int> next(i);
+    std::atomic<bool> stop(false);
+    std::vector<std::thread> pool;
+    const int nt = std::min(nw, j - i);
+    for (int k = 0; k < nt; ++k)
+      pool.emplace_back([&, k]() {
+        bsmpo_ctx* w = h->workers[k];
+        cudaSetDevice(h->device);
+        while (!stop.load()) {
+          const int b = next.fetch_add(1);
+          if (b >= j) break;
+          const int r = bs_update_impl(w, modes[b], u3 + (size_t)b * d3);
+          if (r) {
+            std::lock_guard<std::mutex> lock(err_mutex);
+            if (!err_code) { err_code = r; err_msg = w->err; }
+            stop.store(true);
+            break;
+          }
+          w->last_index = b;
+        }
+        const cudaError_t e = cudaStreamSynchronize(w->stream);
+        if (e != cudaSuccess) {
+          std::lock_guard<std::mutex> lock(err_mutex);
+          if (!err_code) { err_code = BSMPO_ECUDA; err_msg = cudaGetErrorString(e); }
+        }
+      });
+    for (auto& t : pool) t.join();
+    if (err_code) return fail(h, err_code, err_msg);
+    i = j;
+  }
+  // counters and the last update's diagnostics
+  int best = -1;
+  for (int k = 0; k < nw; ++k) {
+    bsmpo_ctx* w = h->workers[k];
+    h->launches += w->launches;
+    h->updates += w->updates;
+    h->jacobi_rounds += w->jacobi_rounds;
+    h->jac_ms += w->jac_ms;
+    h->jac_flops += w->jac_flops;
+    h->jac_launches += w->jac_launches;
+    for (int q = 0; q < 8; ++q) h->stage_ms[q] += w->stage_ms[q];
+    w->launches = w->updates = w->jacobi_rounds = w->jac_launches = 0;
+    w->jac_ms = w->jac_flops = 0.0;
+    for (int q = 0; q < 8; ++q) w->stage_ms[q] = 0.0;
+    if (w->last_index > best) { best = w->last_index; h->diag = w; }
+  }
+  return BSMPO_OK;
 }
 
 int env_all(bsmpo_ctx* h) {
@@ -749,24 +887,27 @@ int bsmpo_create(int n, int d, int chi, int flags, bsmpo_ctx** out) {
   h->profile = prof && prof[0] == '1';
   const char* jr = std::getenv("BSMPO_JACOBI_ROWS");
   if (jr && std::atoi(jr) >= 16) h->jac_rows = std::atoi(jr);
+  const char* nwk = std::getenv("BSMPO_WORKERS");
+  if (nwk && std::atoi(nwk) >= 1 && std::atoi(nwk) <= 64) h->n_workers = std::atoi(nwk);
   *out = h;
   return BSMPO_OK;
 }
 
 int bsmpo_destroy(bsmpo_ctx* h) {
   if (!h) return BSMPO_OK;
+  for (bsmpo_ctx* w : h->workers) destroy_worker(w);
+  h->workers.clear();
   cudaStreamSynchronize(h->stream);
-  DevBuf* bufs[] = {&h->theta, &h->cbuf, &h->abuf, &h->wbuf, &h->vbuf, &h->sig, &h->keys,
-                    &h->perm, &h->tab, &h->tab2, &h->rot, &h->kept, &h->u3, &h->m4,
-                    &h->env_l, &h->env_r, &h->part, &h->outv, &h->dims, &h->nf2, &h->qbuf,
-                    &h->qflag, &h->pbuf, &h->pcnt};
-  for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
-  HostStage* hs[] = {&h->stage, &h->stage2, &h->hres};
-  for (HostStage* b : hs) if (b->p) cudaFreeHost(b->p);
-  if (h->ev0) cudaEventDestroy(h->ev0);
-  if (h->ev1) cudaEventDestroy(h->ev1);
+  free_workspaces(h);
   cudaFree(h->gamma); cudaFree(h->lam); cudaFree(h->charge);
   delete h;
+  return BSMPO_OK;
+}
+
+int bsmpo_set_workers(bsmpo_ctx* h, int n_workers) {
+  if (!h) return fail(nullptr, BSMPO_EINVAL, "null handle");
+  if (n_workers < 1 || n_workers > 64) return fail(h, BSMPO_EINVAL, "workers must be 1..64");
+  h->n_workers = n_workers;
   return BSMPO_OK;
 }
 
@@ -849,6 +990,7 @@ int bsmpo_store_state(bsmpo_ctx* h, void* gamma, double* lambda, int* charge) {
 
 int bsmpo_bs_update_tensor(bsmpo_ctx* h, int mode, const void* u) {
   if (!u) return fail(h, BSMPO_EINVAL, "null tensor");
+  if (h) h->diag = nullptr;
   return bs_update_impl(h, mode, reinterpret_cast<const cplx*>(u));
 }
 
@@ -859,6 +1001,7 @@ int bsmpo_bs_update(bsmpo_ctx* h, int mode, const double* S) {
   const int d = h->d;
   if ((rc = grow(h, h->u3, (size_t)d * d * d * sizeof(cplx)))) return rc;
   CKL(h, launch_fock_tensor_single(d, transpose_to_m8(S), h->u3.p, nullptr, h->stream));
+  h->diag = nullptr;
   return bs_update_impl(h, mode, reinterpret_cast<const cplx*>(h->u3.p));
 }
 
@@ -885,8 +1028,11 @@ int bsmpo_run_mesh(bsmpo_ctx* h, int n_bs, const int* modes, const double* theta
   std::memcpy(h->stage2.p, m4.data(), m4.size() * sizeof(double));
   CK(h, cudaMemcpyAsync(h->m4.p, h->stage2.p, m4.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CKL(h, launch_fock_tensor(d, n_bs, reinterpret_cast<const double*>(h->m4.p), h->u3.p, h->stream));
-  // the stage is reused by the updates: make sure the copy has been consumed
+  // the stage is reused by the updates, and worker streams read u3: drain the stream
   CK(h, cudaStreamSynchronize(h->stream));
+  const int nw = std::min(h->n_workers, n_bs);
+  if (nw > 1) return run_mesh_concurrent(h, n_bs, modes, reinterpret_cast<const cplx*>(h->u3.p), nw);
+  h->diag = nullptr;
   for (int i = 0; i < n_bs; ++i) {
     rc = bs_update_impl(h, modes[i], reinterpret_cast<const cplx*>(h->u3.p) + (size_t)i * d3);
     if (rc) return rc;
@@ -935,8 +1081,9 @@ int bsmpo_observables(bsmpo_ctx* h, double* trace, double* marginals) {
 int bsmpo_last_update_info(const bsmpo_ctx* hc, int* n_sectors, int* sector_cc, int* shape,
                            int* sigma_len, double* sigma, int sigma_cap, int* kept,
                            double* trunc_weight) {
-  bsmpo_ctx* h = const_cast<bsmpo_ctx*>(hc);
-  if (!h) return fail(nullptr, BSMPO_EINVAL, "null handle");
+  if (!hc) return fail(nullptr, BSMPO_EINVAL, "null handle");
+  // after a concurrent mesh the last update's data live in the worker that ran it
+  bsmpo_ctx* h = const_cast<bsmpo_ctx*>(hc->diag ? hc->diag : hc);
   const int ns = h->last_ns;
   if (n_sectors) *n_sectors = ns;
   if (sector_cc) std::copy(h->last_cc.begin(), h->last_cc.end(), sector_cc);
@@ -947,16 +1094,17 @@ int bsmpo_last_update_info(const bsmpo_ctx* hc, int* n_sectors, int* sector_cc, 
   if (sigma) {
     int64_t tot = 0;
     for (int k : h->last_k) tot += k;
-    if (tot > sigma_cap) return fail(h, BSMPO_ECAPACITY, "sigma buffer too small");
+    if (tot > sigma_cap) return fail(const_cast<bsmpo_ctx*>(hc), BSMPO_ECAPACITY, "sigma buffer too small");
     CK(h, cudaMemcpyAsync(sigma, h->sig.p, tot * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
   }
   return BSMPO_OK;
 }
 
-int bsmpo_last_update_work(const bsmpo_ctx* h, double* gemm_flops, double* svd_flops,
+int bsmpo_last_update_work(const bsmpo_ctx* hc, double* gemm_flops, double* svd_flops,
                            double* min_bytes) {
-  if (!h) return fail(nullptr, BSMPO_EINVAL, "null handle");
+  if (!hc) return fail(nullptr, BSMPO_EINVAL, "null handle");
+  const bsmpo_ctx* h = hc->diag ? hc->diag : hc;
   if (gemm_flops) *gemm_flops = h->last_gemm;
   if (svd_flops) *svd_flops = h->last_svd;
   if (min_bytes) *min_bytes = h->last_bytes;

@@ -567,14 +567,11 @@ cudaError_t launch_jacobi_round(const SectorDesc* sd_dev, const JacobiWork* work
                                 const double* nf2, double tol, int max_sweeps, void* pbuf,
                                 int* pcnt, void* qbuf, int* qflag, cudaStream_t s) {
   if (gram_ctas <= 0) return cudaSuccess;
-  static bool attr_done = false;
   const int smem1 = (int)sizeof(GramSmem);
-  if (!attr_done) {
-    cudaError_t e = cudaFuncSetAttribute(jacobi_gram_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem1);
-    if (e != cudaSuccess) return e;
-    attr_done = true;
-  }
+  // once per process (thread-safe initialisation; several host threads launch rounds)
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      jacobi_gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GramSmem));
+  if (attr != cudaSuccess) return attr;
   jacobi_gram_kernel<<<gram_ctas, JNT, smem1, s>>>(
       sd_dev, work_dev, n_work, t, reinterpret_cast<const cplx*>(abuf), rot_count, nf2, tol,
       max_sweeps, reinterpret_cast<cplx*>(pbuf), pcnt, reinterpret_cast<cplx*>(qbuf), qflag);

@@ -111,6 +111,10 @@ class MPOSimulator:
     def set_cutoff(self, cutoff):
         self._chk(self.L.bsmpo_set_cutoff(self.h, float(cutoff)))
 
+    def set_workers(self, n_workers):
+        """Beam splitters of one brick-wall layer that ``run_mesh`` runs at once."""
+        self._chk(self.L.bsmpo_set_workers(self.h, int(n_workers)))
+
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:
             self.L.bsmpo_destroy(self.h)

@@ -107,9 +107,19 @@ int bsmpo_bs_update_tensor(bsmpo_ctx* h, int mode, const void* u);
 
 /* Run a whole mesh (the walk of src/beam_splitter_parallel/Full.py:149-202):
  * n_bs beam splitters T(theta, phi) = [[e^{i phi} cos, -sin], [e^{i phi} sin, cos]]
- * on (modes[i], modes[i]+1), in the given order.  Host arrays. */
+ * on (modes[i], modes[i]+1), in the given order.  Host arrays.  Consecutive entries
+ * whose modes differ pairwise by 2 or more (a brick-wall layer) touch disjoint sites
+ * and run concurrently on the handle's workers (bsmpo_set_workers); the result is the
+ * same as applying them one by one.  Returns with all work complete. */
 int bsmpo_run_mesh(bsmpo_ctx* h, int n_bs, const int* modes, const double* theta,
                    const double* phi);
+
+/* Number of updates bsmpo_run_mesh runs at once (1..64, default 8 or the environment
+ * variable BSMPO_WORKERS at create).  Each worker owns a stream and its own workspaces
+ * (grown on demand, freed by bsmpo_destroy).  Replaces the reference's dispatch of one
+ * layer's beam splitters to separate MPI ranks (src/beam_splitter_parallel/
+ * Full.py:149-166, Rank.py:32-206) within one GPU. */
+int bsmpo_set_workers(bsmpo_ctx* h, int n_workers);
 
 /* Output phase screen exp(i phase_m n_m) on every mode (host double[n]). */
 int bsmpo_apply_phases(bsmpo_ctx* h, const double* phases);

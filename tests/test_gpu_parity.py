@@ -204,6 +204,31 @@ def test_plain_scale_circuit_matches_oracle():
     np.testing.assert_allclose(P.sum(axis=1), np.full(w["n"], tr), atol=1e-12 * abs(tr))
 
 
+def test_concurrent_layers_match_one_by_one():
+    """run_mesh runs a layer's beam splitters on several workers at once; every update
+    computes exactly what it computes alone, so 1 and 4 workers agree bit for bit."""
+    w = circuit.WORKLOADS["plain-small"]
+    U, bs, ph = interferometer.circuit(w["n"], w["seed"])
+    layers = {}
+    for (l, m, th, p) in bs:
+        layers.setdefault(l, []).append((m, th, p))
+    out = []
+    for workers in (1, 4):
+        with engine.MPOSimulator(w["n"], w["d"], w["chi"]) as sim:
+            sim.set_workers(workers)
+            sim.init_single_photons(range(0, w["n"], 2), w["eta"])
+            for l in sorted(layers):
+                ops = layers[l]
+                sim.run_mesh([o[0] for o in ops], [o[1] for o in ops], [o[2] for o in ops])
+            info = sim.last_update_info()
+            g, lam, chg = sim.store()
+            out.append((g.cpu().numpy(), lam.cpu().numpy(), chg.cpu().numpy(), info["kept"]))
+    (g1, l1, c1, k1), (g4, l4, c4, k4) = out
+    assert np.array_equal(c1, c4) and k1 == k4
+    assert np.array_equal(l1, l4)
+    assert np.array_equal(g1, g4)
+
+
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "ref_n*.npz"))),
                          ids=lambda p: os.path.basename(p)[:-4])
 def test_reference_fixtures_on_gpu(path):
