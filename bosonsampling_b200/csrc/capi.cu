@@ -12,6 +12,8 @@
 //   [sync: kept counts] -> V extraction -> W = V^H C grouped GEMM -> scatter.
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
+#include <queue>
 #include <mutex>
 #include <thread>
 #include <chrono>
@@ -52,6 +54,12 @@ struct bsmpo_ctx {
   int n = 0, d = 0, chi = 0;
   int device = 0;
   cudaStream_t stream = nullptr;
+  // workspaces come from this stream-ordered pool (shared with the workers): growing a
+  // buffer never synchronises the device, so other workers' streams keep running
+  cudaMemPool_t pool = nullptr;
+  // host waits of an update sleep on this event (blocking synchronisation) instead of
+  // spinning, so several workers' waits leave the host cores to the launching threads
+  cudaEvent_t wait_ev = nullptr;
   double cutoff = 0.0;
   // device state
   cplx* gamma = nullptr;     // [n][chi][chi]
@@ -105,6 +113,17 @@ int fail(bsmpo_ctx* h, int code, const std::string& msg) {
 // the host mirror of the charge-block sizes (a worker's is its owner's)
 std::vector<int>& mirror(bsmpo_ctx* h) { return h->cnt_shared ? *h->cnt_shared : h->cnt; }
 
+// waits (sleeping) until the handle's stream has drained
+cudaError_t host_wait(bsmpo_ctx* h) {
+  if (!h->wait_ev) {
+    cudaError_t e = cudaEventCreateWithFlags(&h->wait_ev, cudaEventBlockingSync | cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+  }
+  cudaError_t e = cudaEventRecord(h->wait_ev, h->stream);
+  if (e != cudaSuccess) return e;
+  return cudaEventSynchronize(h->wait_ev);
+}
+
 #define CK(h, call)                                                                    \
   do {                                                                                 \
     cudaError_t e_ = (call);                                                           \
@@ -120,14 +139,14 @@ std::vector<int>& mirror(bsmpo_ctx* h) { return h->cnt_shared ? *h->cnt_shared :
 
 int grow(bsmpo_ctx* h, DevBuf& b, size_t bytes) {
   if (bytes <= b.bytes) return BSMPO_OK;
-  // the stream may still use the old buffer
-  CK(h, cudaStreamSynchronize(h->stream));
-  if (b.p) CK(h, cudaFree(b.p));
+  // stream-ordered: the old buffer is released after the stream's earlier work on it
+  if (b.p) CK(h, cudaFreeAsync(b.p, h->stream));
   b.p = nullptr;
   b.bytes = 0;
   size_t want = align_up(bytes + bytes / 4 + 256, 256);
-  if (cudaMalloc(&b.p, want) != cudaSuccess) {
+  if (cudaMallocFromPoolAsync(&b.p, want, h->pool, h->stream) != cudaSuccess) {
     cudaGetLastError();
+    b.p = nullptr;
     return fail(h, BSMPO_ENOMEM, "device allocation of " + std::to_string(want) + " bytes failed");
   }
   b.bytes = want;
@@ -140,7 +159,8 @@ int grow_host(bsmpo_ctx* h, HostStage& b, size_t bytes) {
   if (b.p) CK(h, cudaFreeHost(b.p));
   b.p = nullptr;
   b.bytes = 0;
-  size_t want = align_up(bytes + bytes / 4 + 256, 256);
+  // pinned host memory: rare, generous growth (allocation and release are synchronous)
+  size_t want = std::max<size_t>(align_up(bytes + bytes / 2 + 256, 256), 1 << 20);
   CK(h, cudaMallocHost(&b.p, want));
   b.bytes = want;
   return BSMPO_OK;
@@ -484,7 +504,7 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
       h->launches += 2;
     }
     CK(h, cudaMemcpyAsync(hrot, h->rot.p, (size_t)3 * ns * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(h, cudaStreamSynchronize(st));
+    CK(h, host_wait(h));
     ++checks;
     bool all = true;
     for (int s = 0; s < ns; ++s) {
@@ -570,7 +590,7 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   double* htw = reinterpret_cast<double*>(static_cast<char*>(h->hres.p) + 512);
   CK(h, cudaMemcpyAsync(hk, kept_d, (size_t)(ns + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(h, cudaMemcpyAsync(htw, trunc_d, sizeof(double), cudaMemcpyDeviceToHost, st));
-  CK(h, cudaStreamSynchronize(st));
+  CK(h, host_wait(h));
   const int total_kept = hk[ns];
   if ((rc = clk.mark(4))) return rc;
   // 5. V and W = V^H C
@@ -670,12 +690,14 @@ void free_workspaces(bsmpo_ctx* h) {
                     &h->env_l, &h->env_r, &h->part, &h->outv, &h->dims, &h->nf2, &h->qbuf,
                     &h->qflag, &h->pbuf, &h->pcnt};
   for (DevBuf* b : bufs)
-    if (b->p) cudaFree(b->p);
+    if (b->p) cudaFreeAsync(b->p, h->stream);
+  cudaStreamSynchronize(h->stream);
   HostStage* hs[] = {&h->stage, &h->stage2, &h->hres};
   for (HostStage* b : hs)
     if (b->p) cudaFreeHost(b->p);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->wait_ev) cudaEventDestroy(h->wait_ev);
 }
 
 // A worker context for concurrent updates: the owner's state, its own stream.
@@ -683,6 +705,7 @@ int make_worker(bsmpo_ctx* h, bsmpo_ctx** out) {
   bsmpo_ctx* w = new bsmpo_ctx();
   w->n = h->n; w->d = h->d; w->chi = h->chi; w->device = h->device;
   w->gamma = h->gamma; w->lam = h->lam; w->charge = h->charge;
+  w->pool = h->pool;
   w->loaded = true;
   w->cnt_shared = &h->cnt;
   w->profile = h->profile;
@@ -702,10 +725,13 @@ void destroy_worker(bsmpo_ctx* w) {
   delete w;   // the state belongs to the owner
 }
 
-// Runs the updates of a mesh on the owner's workers: consecutive beam splitters whose
-// modes differ by 2 or more pairwise (one brick-wall layer) touch disjoint sites and
-// write disjoint bonds, so they run concurrently, one per worker stream; a layer ends
-// with every worker's stream drained (host barrier) before the next one starts.  Every
+// Runs the updates of a mesh on the owner's workers.  Two beam splitters conflict when
+// their modes differ by 0 or 1 (shared site); update k depends on the latest earlier
+// update at modes m_k - 1, m_k and m_k + 1 -- nothing else it touches is written by
+// another update (modes 2 apart share only a bond both read).  Workers take the
+// lowest-numbered update whose dependencies have finished (host side: after their
+// host mirror entries are written; device side: the worker's stream waits for the
+// events recorded at their ends), so consecutive brick-wall layers overlap.  Every
 // update computes exactly what it computes alone.
 int run_mesh_concurrent(bsmpo_ctx* h, int n_bs, const int* modes, const cplx* u3, int nw) {
   const int d3 = h->d * h->d * h->d;
@@ -726,46 +752,81 @@ int run_mesh_concurrent(bsmpo_ctx* h, int n_bs, const int* modes, const cplx* u3
     }
     w->last_index = -1;
   }
-  std::mutex err_mutex;
+  // dependencies
+  std::vector<int> pred((size_t)3 * n_bs, -1), remaining(n_bs, 0);
+  std::vector<std::vector<int>> succ(n_bs);
+  {
+    std::vector<int> last(h->n, -1);
+    for (int k = 0; k < n_bs; ++k) {
+      const int m = modes[k];
+      int c = 0;
+      for (int dm = -1; dm <= 1; ++dm) {
+        const int mm = m + dm;
+        if (mm < 0 || mm > h->n - 2 || last[mm] < 0) continue;
+        pred[(size_t)3 * k + c++] = last[mm];
+        succ[last[mm]].push_back(k);
+      }
+      remaining[k] = c;
+      last[m] = k;
+    }
+  }
+  std::vector<cudaEvent_t> done_ev(n_bs, nullptr);
+  for (int k = 0; k < n_bs; ++k)
+    if (cudaEventCreateWithFlags(&done_ev[k], cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      for (cudaEvent_t e : done_ev) if (e) cudaEventDestroy(e);
+      return fail(h, BSMPO_ECUDA, "event creation failed");
+    }
+  std::mutex mu;
+  std::condition_variable cv;
+  std::priority_queue<int, std::vector<int>, std::greater<int>> ready;
+  for (int k = 0; k < n_bs; ++k)
+    if (remaining[k] == 0) ready.push(k);
+  int finished = 0;
   int err_code = BSMPO_OK;
   std::string err_msg;
-  for (int i = 0; i < n_bs;) {
-    int j = i + 1;
-    for (; j < n_bs; ++j) {
-      bool ok = true;
-      for (int l = i; l < j && ok; ++l) ok = std::abs(modes[j] - modes[l]) >= 2;
-      if (!ok) break;
-    }
-    std::atomic<int> next(i);
-    std::atomic<bool> stop(false);
-    std::vector<std::thread> pool;
-    const int nt = std::min(nw, j - i);
-    for (int k = 0; k < nt; ++k)
-      pool.emplace_back([&, k]() {
-        bsmpo_ctx* w = h->workers[k];
-        cudaSetDevice(h->device);
-        while (!stop.load()) {
-          const int b = next.fetch_add(1);
-          if (b >= j) break;
-          const int r = bs_update_impl(w, modes[b], u3 + (size_t)b * d3);
-          if (r) {
-            std::lock_guard<std::mutex> lock(err_mutex);
-            if (!err_code) { err_code = r; err_msg = w->err; }
-            stop.store(true);
-            break;
-          }
-          w->last_index = b;
+  std::vector<std::thread> pool;
+  for (int wk = 0; wk < nw; ++wk)
+    pool.emplace_back([&, wk]() {
+      bsmpo_ctx* w = h->workers[wk];
+      cudaSetDevice(h->device);
+      for (;;) {
+        int k;
+        {
+          std::unique_lock<std::mutex> lock(mu);
+          cv.wait(lock, [&] { return err_code || finished == n_bs || !ready.empty(); });
+          if (err_code || ready.empty()) break;
+          k = ready.top();
+          ready.pop();
         }
-        const cudaError_t e = cudaStreamSynchronize(w->stream);
-        if (e != cudaSuccess) {
-          std::lock_guard<std::mutex> lock(err_mutex);
-          if (!err_code) { err_code = BSMPO_ECUDA; err_msg = cudaGetErrorString(e); }
+        int r = BSMPO_OK;
+        for (int c = 0; c < 3 && !r; ++c) {
+          const int j = pred[(size_t)3 * k + c];
+          if (j >= 0 && cudaStreamWaitEvent(w->stream, done_ev[j], 0) != cudaSuccess)
+            r = fail(w, BSMPO_ECUDA, "cudaStreamWaitEvent failed");
         }
-      });
-    for (auto& t : pool) t.join();
-    if (err_code) return fail(h, err_code, err_msg);
-    i = j;
+        if (!r) r = bs_update_impl(w, modes[k], u3 + (size_t)k * d3);
+        if (!r && cudaEventRecord(done_ev[k], w->stream) != cudaSuccess)
+          r = fail(w, BSMPO_ECUDA, "cudaEventRecord failed");
+        std::lock_guard<std::mutex> lock(mu);
+        if (r) {
+          if (!err_code) { err_code = r; err_msg = w->err; }
+        } else {
+          w->last_index = std::max(w->last_index, k);
+          ++finished;
+          for (int s2 : succ[k])
+            if (--remaining[s2] == 0) ready.push(s2);
+        }
+        cv.notify_all();
+      }
+    });
+  for (auto& t : pool) t.join();
+  for (int wk = 0; wk < nw; ++wk) {
+    const cudaError_t e = host_wait(h->workers[wk]);
+    if (e != cudaSuccess && !err_code) { err_code = BSMPO_ECUDA; err_msg = cudaGetErrorString(e); }
   }
+  for (cudaEvent_t e : done_ev) cudaEventDestroy(e);
+  if (err_code) return fail(h, err_code, err_msg);
   // counters and the last update's diagnostics
   int best = -1;
   for (int k = 0; k < nw; ++k) {
@@ -882,6 +943,19 @@ int bsmpo_create(int n, int d, int chi, int flags, bsmpo_ctx** out) {
     delete h;
     return fail(nullptr, BSMPO_ENOMEM, "state allocation failed");
   }
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = h->device;
+  if (cudaMemPoolCreate(&h->pool, &props) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(h->gamma); cudaFree(h->lam); cudaFree(h->charge);
+    delete h;
+    return fail(nullptr, BSMPO_ECUDA, "memory pool creation failed");
+  }
+  // keep released workspace memory in the pool (no release at synchronisation points)
+  uint64_t keep = UINT64_MAX;
+  cudaMemPoolSetAttribute(h->pool, cudaMemPoolAttrReleaseThreshold, &keep);
   h->cnt.assign((size_t)(n + 1) * d * d, 0);
   const char* prof = std::getenv("BSMPO_PROFILE");
   h->profile = prof && prof[0] == '1';
@@ -899,6 +973,7 @@ int bsmpo_destroy(bsmpo_ctx* h) {
   h->workers.clear();
   cudaStreamSynchronize(h->stream);
   free_workspaces(h);
+  if (h->pool) cudaMemPoolDestroy(h->pool);
   cudaFree(h->gamma); cudaFree(h->lam); cudaFree(h->charge);
   delete h;
   return BSMPO_OK;
