@@ -402,8 +402,9 @@ __global__ __launch_bounds__(JNT) void jacobi_gram_kernel(const SectorDesc* __re
 
 // Round kernel 2: every part of a rotated pair applies Q to its rows on the FP64 tensor
 // path, straight from global memory into mma fragments: warp w owns rows
-// [16 w, 16 w + 16) (two 8-row tiles) x the four 8-column tiles;
-// (tr + i ti)(qr + i qi) = (tr qr - ti qi) + i (tr qi + ti qr)
+// [16 w, 16 w + 16), one 8-row tile at a time, x the four 8-column tiles.  The complex
+// product takes three real products (Gauss):
+// (tr + i ti)(qr + i qi) = (tr qr - ti qi) + i ((tr + ti)(qr + qi) - tr qr - ti qi).
 __global__ __launch_bounds__(JNT) void jacobi_apply_kernel(const SectorDesc* __restrict__ sd,
                                                            const JacobiWork* __restrict__ work,
                                                            int n_work, int t, cplx* __restrict__ abuf,
@@ -411,6 +412,7 @@ __global__ __launch_bounds__(JNT) void jacobi_apply_kernel(const SectorDesc* __r
                                                            const cplx* __restrict__ qbuf,
                                                            const int* __restrict__ qflag) {
   __shared__ double2 Qs[JC][JC + 1];
+  __shared__ double Qsum[JC][JC + 1];   // Re Q + Im Q
   __shared__ int cols[JC];
   const int tid = threadIdx.x;
   const JacTask T = jac_task(work, n_work, t, true);
@@ -427,51 +429,51 @@ __global__ __launch_bounds__(JNT) void jacobi_apply_kernel(const SectorDesc* __r
     const int e = tid + i * JNT;
     const cplx v = ldc(qi + e);
     Qs[e / JC][e % JC] = make_double2(v.x, v.y);
+    Qsum[e / JC][e % JC] = v.x + v.y;
   }
   __syncthreads();
   cplx* A = abuf + D.a_off;
   const int warp = tid >> 5, lane = tid & 31, li = lane >> 2, lk = lane & 3;
   if (16 * warp >= nr) return;
-  double2 tv[2][JC / 4];
-#pragma unroll
+#pragma unroll 1
   for (int a = 0; a < 2; ++a) {
     const int row = 16 * warp + 8 * a + li;
+    double2 tv[JC / 4];
 #pragma unroll
     for (int kk = 0; kk < JC / 4; ++kk) {
       const int col = cols[4 * kk + lk];
-      tv[a][kk] = make_double2(0.0, 0.0);
-      if (row < nr && col >= 0) tv[a][kk] = *reinterpret_cast<const double2*>(A + (int64_t)(r0 + row) * k + col);
+      tv[kk] = make_double2(0.0, 0.0);
+      if (row < nr && col >= 0) tv[kk] = *reinterpret_cast<const double2*>(A + (int64_t)(r0 + row) * k + col);
     }
-  }
-  double2 ore[2][4], oim[2][4];
-#pragma unroll
-  for (int a = 0; a < 2; ++a)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) { ore[a][c] = make_double2(0, 0); oim[a][c] = make_double2(0, 0); }
-#pragma unroll
-  for (int kk = 0; kk < JC / 4; ++kk) {
-    double2 q[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) q[c] = Qs[4 * kk + lk][8 * c + li];
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        dmma(ore[a][c], tv[a][kk].x, q[c].x);
-        dmma(ore[a][c], -tv[a][kk].y, q[c].y);
-        dmma(oim[a][c], tv[a][kk].x, q[c].y);
-        dmma(oim[a][c], tv[a][kk].y, q[c].x);
-      }
-  }
-#pragma unroll
-  for (int a = 0; a < 2; ++a) {
-    const int row = 16 * warp + 8 * a + li;
-    if (row >= nr) continue;
+    // t1 = Tr Qr, t2 = Ti Qi, t3 = (Tr + Ti)(Qr + Qi) on the four column tiles
+    double2 t1[4], t2[4], t3[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const int c0 = cols[8 * c + 2 * lk], c1 = cols[8 * c + 2 * lk + 1];
-      if (c0 >= 0) stc(A + (int64_t)(r0 + row) * k + c0, cmake(ore[a][c].x, oim[a][c].x));
-      if (c1 >= 0) stc(A + (int64_t)(r0 + row) * k + c1, cmake(ore[a][c].y, oim[a][c].y));
+      t1[c] = make_double2(0, 0);
+      t2[c] = make_double2(0, 0);
+      t3[c] = make_double2(0, 0);
+    }
+#pragma unroll
+    for (int kk = 0; kk < JC / 4; ++kk) {
+      const double ts = tv[kk].x + tv[kk].y;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const double2 q = Qs[4 * kk + lk][8 * c + li];
+        const double qs = Qsum[4 * kk + lk][8 * c + li];
+        dmma(t1[c], tv[kk].x, q.x);
+        dmma(t2[c], tv[kk].y, q.y);
+        dmma(t3[c], ts, qs);
+      }
+    }
+    if (row < nr) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int c0 = cols[8 * c + 2 * lk], c1 = cols[8 * c + 2 * lk + 1];
+        if (c0 >= 0)
+          stc(A + (int64_t)(r0 + row) * k + c0, cmake(t1[c].x - t2[c].x, t3[c].x - t1[c].x - t2[c].x));
+        if (c1 >= 0)
+          stc(A + (int64_t)(r0 + row) * k + c1, cmake(t1[c].y - t2[c].y, t3[c].y - t1[c].y - t2[c].y));
+      }
     }
   }
 }
