@@ -153,6 +153,23 @@ class ClockSampler:
                 "source": "nvml" if self._nvml else "nvidia-smi"}
 
 
+def max_over_ranks(x, dist, device):
+    """The largest x over the ranks of the process group (x itself on one rank): every
+    multi-rank time is the slowest rank's."""
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(n_units_per_rank, world, seconds):
+    """Whole-job rate of `world` replicas that each process n_units_per_rank units, timed
+    as the slowest rank's seconds (weak scaling)."""
+    return world * n_units_per_rank / seconds
+
+
 def layers_of(bs):
     n_layers = max(b[0] for b in bs) + 1
     out = [[] for _ in range(n_layers)]
@@ -318,13 +335,10 @@ def main():
     launches = sim.kernel_launches() - launches0
     jac_ms, jac_flops, jac_launches = sim.jacobi_timing()
     sim.set_timing(False)
-    t_dev = e0.elapsed_time(e1) / 1e3
+    t_dev = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, "cuda")
     if world > 1:
-        t = torch.tensor([t_dev], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_dev = float(t.item())
         dist.barrier()
-    value = world * n_bs / t_dev
+    value = replica_rate(n_bs, world, t_dev)
 
     # ---- end to end through the public API with host buffers: per step the state is
     # copied host -> device and loaded, the layer runs, the state is stored and copied
@@ -348,11 +362,7 @@ def main():
         g_out.copy_(g1, non_blocking=True)
         tr = sim.trace()
     torch.cuda.synchronize()
-    t_e2e = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    t_e2e = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
     n_bs_e2e = sum(len(layers[args.start_layer + i]) for i in range(e2e_steps))
     h2d = (g_host.numel() * 16 + l_host.numel() * 8 + c_host.numel() * 4) * e2e_steps
     d2h = (g_out.numel() * 16 + 16) * e2e_steps
@@ -388,7 +398,7 @@ def main():
                        "l2": "inputs larger than L2 (state %.2f GB)" % (g_host.numel() * 16 / 1e9),
                        "bs_slice": args.bs_slice or "whole layer",
                        "cutoff": 0.0},
-            "e2e": {"value": world * n_bs_e2e / t_e2e, "unit": "BS-updates/s",
+            "e2e": {"value": replica_rate(n_bs_e2e, world, t_e2e), "unit": "BS-updates/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
             "roofline": {"kernel": "jacobi_gram_kernel + jacobi_apply_kernel (one-sided Jacobi SVD rounds)",
