@@ -60,6 +60,7 @@ struct bsmpo_ctx {
   // host waits of an update sleep on this event (blocking synchronisation) instead of
   // spinning, so several workers' waits leave the host cores to the launching threads
   cudaEvent_t wait_ev = nullptr;
+  cudaEvent_t poll_ev[2] = {nullptr, nullptr};   // Jacobi convergence polls (blocking sync)
   double cutoff = 0.0;
   // device state
   cplx* gamma = nullptr;     // [n][chi][chi]
@@ -446,7 +447,7 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   const TabLayout L = layout_of(P);
   if ((rc = grow(h, h->tab, L.total))) return rc;
   if ((rc = grow_host(h, h->stage, L.total))) return rc;
-  if ((rc = grow_host(h, h->hres, 4096 + (size_t)(ns + 2) * sizeof(int) + 3 * ns * sizeof(int)))) return rc;
+  if ((rc = grow_host(h, h->hres, 4096 + (size_t)(ns + 2) * sizeof(int) + 6 * ns * sizeof(int)))) return rc;
   char* hs = static_cast<char*>(h->stage.p);
   std::memcpy(hs + L.tab, &P.tab, sizeof(UpdateTables));
   put(hs, L.tidx, P.tidx);
@@ -485,16 +486,26 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   CKL(h, launch_sector_norms(sd_d, ns, h->abuf.p, nf2, st));
   CK(h, cudaMemsetAsync(h->rot.p, 0, (size_t)3 * ns * sizeof(int), st));
   CK(h, cudaMemsetAsync(h->pcnt.p, 0, std::max(P.jac_slots, 1) * sizeof(int), st));
-  int* hrot = reinterpret_cast<int*>(static_cast<char*>(h->hres.p) + 1024);
+  // Convergence polls run one chunk behind: after launching chunk c + 1 the host reads
+  // the counters copied after chunk c, so the stream always has a chunk queued while the
+  // host checks (a converged sector's rounds in the extra chunk exit at once).  Counters
+  // and compacted launch tables alternate between two pinned slots.
+  int* hrot_slot[2] = {reinterpret_cast<int*>(static_cast<char*>(h->hres.p) + 1024), nullptr};
+  hrot_slot[1] = hrot_slot[0] + 3 * ns;
+  const size_t jw_bytes = align_up(std::max<size_t>(P.jw.size(), 1) * sizeof(JacobiWork), 256);
+  if ((rc = grow_host(h, h->stage2, 2 * jw_bytes))) return rc;
+  char* jw_stage[2] = {static_cast<char*>(h->stage2.p), static_cast<char*>(h->stage2.p) + jw_bytes};
+  for (cudaEvent_t& e : h->poll_ev)
+    if (!e) CK(h, cudaEventCreateWithFlags(&e, cudaEventBlockingSync | cudaEventDisableTiming));
   int t = 0;
   const int t_max = MAX_SWEEPS * std::max(1, P.max_rounds);
   bool converged = false;
   int checks = 0;
   std::vector<int> conv_at(ns, -1);
   if (h->timing) CK(h, cudaEventRecord(h->ev0, st));
-  while (t < t_max) {
-    // run one sweep of the largest sector, then test convergence
-    const int chunk = std::max(1, P.max_rounds);
+  const int chunk = std::max(1, P.max_rounds);   // one sweep of the largest sector
+  int t_after[2] = {0, 0};
+  auto launch_chunk = [&](int slot) -> int {
     for (int i = 0; i < chunk && t < t_max; ++i, ++t) {
       // tol <= 0: per-sector default 4 eps sqrt(rows of the Gram), at least 8 eps
       CK(h, launch_jacobi_round(sd_d, jw_d, (int)active.size(), gram_ctas, apply_ctas, t,
@@ -503,31 +514,45 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
                                 reinterpret_cast<int*>(h->qflag.p), st));
       h->launches += 2;
     }
-    CK(h, cudaMemcpyAsync(hrot, h->rot.p, (size_t)3 * ns * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(h, host_wait(h));
+    CK(h, cudaMemcpyAsync(hrot_slot[slot], h->rot.p, (size_t)3 * ns * sizeof(int),
+                          cudaMemcpyDeviceToHost, st));
+    CK(h, cudaEventRecord(h->poll_ev[slot], st));
+    t_after[slot] = t;
+    return BSMPO_OK;
+  };
+  if ((rc = launch_chunk(0))) return rc;
+  int cur = 0, compactions = 0;
+  for (;;) {
+    const bool more = t < t_max;
+    if (more && (rc = launch_chunk(cur ^ 1))) return rc;
+    CK(h, cudaEventSynchronize(h->poll_ev[cur]));
     ++checks;
+    const int* hrot = hrot_slot[cur];
     bool all = true;
     for (int s = 0; s < ns; ++s) {
       // a converged sector leaves the launches, and its counters are stale from then on
       if (conv_at[s] >= 0) continue;
       const int R = P.jw[s].rounds;
-      const int done = t / R;
+      const int done = t_after[cur] / R;
       if (done < 1 || hrot[3 * s + (done - 1) % 3] != 0) { all = false; continue; }
       conv_at[s] = done;
     }
     if (all) { converged = true; break; }
-    // drop converged sectors (and those out of sweeps) from the next rounds' launches;
-    // the stream is idle, so the pinned stage and the device table are free
+    if (!more) break;
+    // drop converged sectors (and those out of sweeps) from the launches after the queued
+    // chunk: the table copy is stream-ordered after it
     std::vector<JacobiWork> next;
     for (const auto& w : P.jw)
       if (conv_at[w.sector] < 0 && t / w.rounds < MAX_SWEEPS) next.push_back(w);
     if (next.size() < active.size() && !next.empty()) {
       active.swap(next);
       jacobi_launch_list(active, &gram_ctas, &apply_ctas, &slots);
-      put(hs, L.jw, active);
-      CK(h, cudaMemcpyAsync(dt + L.jw, hs + L.jw, active.size() * sizeof(JacobiWork),
+      char* stg = jw_stage[compactions++ & 1];
+      put(stg, 0, active);
+      CK(h, cudaMemcpyAsync(dt + L.jw, stg, active.size() * sizeof(JacobiWork),
                             cudaMemcpyHostToDevice, st));
     }
+    cur ^= 1;
   }
   if (h->timing) CK(h, cudaEventRecord(h->ev1, st));
   h->last_sweeps = t / std::max(1, P.max_rounds);
@@ -552,12 +577,12 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   if (!converged) {
     std::string msg = "Jacobi SVD did not converge (mode " + std::to_string(mode) + ")";
     for (int s = 0; s < ns; ++s) {
-      const int R = P.jw[s].rounds, done = t / R;
+      const int R = P.jw[s].rounds, done = t_after[cur] / R;
       if (conv_at[s] >= 0) continue;
       const SectorDesc& S = P.sd[s];
       msg += "; sector (" + std::to_string(S.cc0) + "," + std::to_string(S.cc1) + ") m=" +
              std::to_string(S.m) + " n=" + std::to_string(S.n) + " sweeps=" + std::to_string(done) +
-             " rotations=" + std::to_string(hrot[3 * s + (done - 1 + 3) % 3]);
+             " rotations=" + std::to_string(hrot_slot[cur][3 * s + (done - 1 + 3) % 3]);
       const char* dump = std::getenv("BSMPO_DEBUG_DUMP");
       if (dump && dump[0]) {
         // the sector's C (row-major m x n complex128) followed by Lambda_R of its columns
@@ -698,6 +723,8 @@ void free_workspaces(bsmpo_ctx* h) {
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->wait_ev) cudaEventDestroy(h->wait_ev);
+  for (cudaEvent_t& e : h->poll_ev)
+    if (e) cudaEventDestroy(e);
 }
 
 // A worker context for concurrent updates: the owner's state, its own stream.
