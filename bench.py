@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--start-layer", type=int, default=10)
     p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work per sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-circuit", action="store_true",
+                   help="skip the whole-circuit run (all updates from the initial state)")
     p.add_argument("--workload", default="chi1024", choices=sorted(WORKLOADS))
     p.add_argument("--bs-slice", default=None,
                    help="profiling runs only: START:STOP -- a step runs beam splitters START..STOP-1 "
@@ -396,6 +398,27 @@ def main():
     h2d = (g_host.numel() * 16 + l_host.numel() * 8 + c_host.numel() * 4) * e2e_steps
     d2h = (g_out.numel() * 16 + 16) * e2e_steps
 
+    # ---- the whole circuit: every update from the initial state, the output phases and
+    # the observables (trace, marginals), in one run_mesh call, on a second handle
+    circuit = None
+    if not args.no_circuit and not args.bs_slice:
+        with engine.MPOSimulator(w["n"], w["d"], w["chi"]) as full:
+            full.init_single_photons(range(0, w["n"], 2), w["eta"])
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            t0 = time.perf_counter()
+            full.run_mesh([b[1] for b in bs], [b[2] for b in bs], [b[3] for b in bs])
+            full.apply_phases(out_phases)
+            trace_c, _ = full.observables()
+            torch.cuda.synchronize()
+            t_circ = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+        circuit = {"bs_updates": len(bs), "seconds": round(t_circ, 3),
+                   "value": replica_rate(len(bs), world, t_circ), "unit": "BS-updates/s",
+                   "trace": float(trace_c.real),
+                   "covers": "all updates from the initial state, output phases, trace and marginals "
+                             "(host wall clock, initial state excluded)"}
+
     # ---- roofline of the dominant kernel (the Jacobi round), FP64 against measured DGEMM
     fp64_peak = measure_fp64_peak(torch) if rank == 0 else None
     cpu = None
@@ -441,6 +464,7 @@ def main():
                          "traffic": 21995008 if args.workload == "chi1024" else None,
                          "traffic_unit": "bytes per launch"},
             "clocks": clocks,
+            "circuit": circuit,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))
