@@ -30,9 +30,12 @@ SIGNATURES = {
     "bsmpo_set_workers": (_c_int, [_vp, _c_int]),
     "bsmpo_load_state": (_c_int, [_vp, _vp, _vp, _vp]),
     "bsmpo_store_state": (_c_int, [_vp, _vp, _vp, _vp]),
+    "bsmpo_init_product": (_c_int, [_vp, _dp, _c_int]),
+    "bsmpo_canonicalize": (_c_int, [_vp]),
     "bsmpo_bs_update": (_c_int, [_vp, _c_int, _dp]),
     "bsmpo_bs_update_tensor": (_c_int, [_vp, _c_int, _vp]),
     "bsmpo_run_mesh": (_c_int, [_vp, _c_int, _ip, _dp, _dp]),
+    "bsmpo_mesh_truncation": (_c_int, [_vp, _dp, _c_int]),
     "bsmpo_apply_phases": (_c_int, [_vp, _dp]),
     "bsmpo_observables": (_c_int, [_vp, _dp, _dp]),
     "bsmpo_last_update_info": (_c_int, [_vp, _ip, _ip, _ip, _ip, _dp, _c_int, _ip, _dp]),

@@ -101,6 +101,7 @@ struct bsmpo_ctx {
   int n_workers = 8;      // BSMPO_WORKERS / bsmpo_set_workers
   const bsmpo_ctx* diag = nullptr;
   int last_index = -1;    // worker: mesh index of the last update it ran
+  std::vector<double> mesh_tw;   // truncation weight of every update of the last mesh
 };
 
 namespace {
@@ -555,8 +556,14 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
     cur ^= 1;
   }
   if (h->timing) CK(h, cudaEventRecord(h->ev1, st));
-  h->last_sweeps = t / std::max(1, P.max_rounds);
-  h->jacobi_rounds += t;
+  // sweeps the slowest sector needed (its last one without rotations included); t also
+  // counts the chunk queued after convergence, whose rounds exit at once
+  {
+    int sw = 0;
+    for (int s = 0; s < ns; ++s) sw = std::max(sw, conv_at[s] >= 0 ? conv_at[s] : t / P.jw[s].rounds);
+    h->last_sweeps = sw;
+  }
+  h->jacobi_rounds += t;   // launched rounds, including the drained chunk
   if (h->timing) {
     float ms = 0.f;
     CK(h, cudaEventSynchronize(h->ev1));
@@ -583,21 +590,6 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
       msg += "; sector (" + std::to_string(S.cc0) + "," + std::to_string(S.cc1) + ") m=" +
              std::to_string(S.m) + " n=" + std::to_string(S.n) + " sweeps=" + std::to_string(done) +
              " rotations=" + std::to_string(hrot_slot[cur][3 * s + (done - 1 + 3) % 3]);
-      const char* dump = std::getenv("BSMPO_DEBUG_DUMP");
-      if (dump && dump[0]) {
-        // the sector's C (row-major m x n complex128) followed by Lambda_R of its columns
-        std::vector<cplx> hc((size_t)S.m * S.n);
-        CK(h, cudaMemcpy(hc.data(), static_cast<cplx*>(h->cbuf.p) + S.c_off,
-                         hc.size() * sizeof(cplx), cudaMemcpyDeviceToHost));
-        FILE* f = std::fopen(dump, "wb");
-        if (f) {
-          int hdr[4] = {S.m, S.n, S.cc0, S.cc1};
-          std::fwrite(hdr, sizeof(int), 4, f);
-          std::fwrite(hc.data(), sizeof(cplx), hc.size(), f);
-          std::fclose(f);
-        }
-        dump = nullptr;
-      }
       break;
     }
     return fail(h, BSMPO_ECONVERGE, msg);
@@ -833,6 +825,7 @@ int run_mesh_concurrent(bsmpo_ctx* h, int n_bs, const int* modes, const cplx* u3
             r = fail(w, BSMPO_ECUDA, "cudaStreamWaitEvent failed");
         }
         if (!r) r = bs_update_impl(w, modes[k], u3 + (size_t)k * d3);
+        if (!r) h->mesh_tw[k] = w->last_trunc;   // each k is written by one worker only
         if (!r && cudaEventRecord(done_ev[k], w->stream) != cudaSuccess)
           r = fail(w, BSMPO_ECUDA, "cudaEventRecord failed");
         std::lock_guard<std::mutex> lock(mu);
@@ -1079,6 +1072,71 @@ int bsmpo_load_state(bsmpo_ctx* h, const void* gamma, const double* lambda, cons
   return BSMPO_OK;
 }
 
+int bsmpo_init_product(bsmpo_ctx* h, const double* rho, int total_photons) {
+  if (!h || !rho) return fail(h, BSMPO_EINVAL, "null argument");
+  const int n = h->n, d = h->d, chi = h->chi, dd = d * d;
+  if (total_photons >= d) return fail(h, BSMPO_EINVAL, "total_photons must be < d (or negative: none)");
+  // bond charges, right to left: (ket, bra) photons right of the bond, at most d - 1
+  std::vector<std::vector<int>> bonds(n + 1);   // flat charge index c0 * d + c1, sorted
+  bonds[n] = {0};
+  std::vector<char> mark(dd);
+  for (int b = n - 1; b >= 0; --b) {
+    std::fill(mark.begin(), mark.end(), 0);
+    if (b == 0) {
+      // every diagonal total, reachable or not (or only the post-selected one)
+      for (int c = 0; c < d; ++c)
+        if (total_photons < 0 || c == total_photons) mark[c * d + c] = 1;
+    } else {
+      const double* r = rho + (size_t)b * dd * 2;
+      for (int q : bonds[b + 1]) {
+        const int c0 = q / d, c1 = q % d;
+        for (int o0 = 0; o0 + c0 < d; ++o0)
+          for (int o1 = 0; o1 + c1 < d; ++o1)
+            if (r[(o0 * d + o1) * 2] != 0.0 || r[(o0 * d + o1) * 2 + 1] != 0.0)
+              mark[(c0 + o0) * d + c1 + o1] = 1;
+      }
+    }
+    for (int q = 0; q < dd; ++q)
+      if (mark[q]) bonds[b].push_back(q);
+    if ((int)bonds[b].size() > chi)
+      return fail(h, BSMPO_ECAPACITY, "chi = " + std::to_string(chi) + " is smaller than the product-state "
+                                      "bond dimension " + std::to_string(bonds[b].size()));
+  }
+  std::vector<int> hc((size_t)(n + 1) * chi * 2, d);
+  std::vector<double> hl((size_t)(n + 1) * chi, 0.0);
+  std::fill(h->cnt.begin(), h->cnt.end(), 0);
+  for (int b = 0; b <= n; ++b)
+    for (size_t i = 0; i < bonds[b].size(); ++i) {
+      const int q = bonds[b][i];
+      hc[((size_t)b * chi + i) * 2] = q / d;
+      hc[((size_t)b * chi + i) * 2 + 1] = q % d;
+      hl[(size_t)b * chi + i] = 1.0;
+      h->cnt[(size_t)b * dd + q]++;
+    }
+  int rc;
+  if ((rc = grow(h, h->m4, (size_t)n * dd * sizeof(cplx)))) return rc;
+  cudaStream_t st = h->stream;
+  CK(h, cudaMemcpyAsync(h->charge, hc.data(), hc.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  CK(h, cudaMemcpyAsync(h->lam, hl.data(), hl.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(h, cudaMemcpyAsync(h->m4.p, rho, (size_t)n * dd * sizeof(cplx), cudaMemcpyHostToDevice, st));
+  CKL(h, launch_product_fill(n, d, chi, h->charge, h->m4.p, h->gamma, st));
+  CK(h, cudaStreamSynchronize(st));
+  h->loaded = true;
+  h->diag = nullptr;
+  return BSMPO_OK;
+}
+
+int bsmpo_canonicalize(bsmpo_ctx* h) {
+  int rc = check_mode(h, 0);
+  if (rc) return rc;
+  // right-to-left sweep of identity-gate updates (the reference's Canonicalize,
+  // src/MPO.py:137-155, whose phase-only gate acts as the identity on product inputs)
+  const double I[8] = {1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0};
+  for (int mode = h->n - 2; mode >= 0; --mode)
+    if ((rc = bsmpo_bs_update(h, mode, I))) return rc;
+  return BSMPO_OK;
+}
+
 int bsmpo_store_state(bsmpo_ctx* h, void* gamma, double* lambda, int* charge) {
   if (!h || !h->loaded) return fail(h, BSMPO_EINVAL, "no state loaded");
   const int n = h->n, chi = h->chi;
@@ -1110,6 +1168,7 @@ int bsmpo_bs_update(bsmpo_ctx* h, int mode, const double* S) {
 int bsmpo_run_mesh(bsmpo_ctx* h, int n_bs, const int* modes, const double* theta, const double* phi) {
   if (!h || n_bs < 0 || (n_bs > 0 && (!modes || !theta || !phi))) return fail(h, BSMPO_EINVAL, "bad argument");
   if (!h->loaded) return fail(h, BSMPO_EINVAL, "no state loaded");
+  h->mesh_tw.assign(n_bs, 0.0);
   if (n_bs == 0) return BSMPO_OK;
   const int d = h->d, d3 = d * d * d;
   int rc;
@@ -1138,8 +1197,18 @@ int bsmpo_run_mesh(bsmpo_ctx* h, int n_bs, const int* modes, const double* theta
   for (int i = 0; i < n_bs; ++i) {
     rc = bs_update_impl(h, modes[i], reinterpret_cast<const cplx*>(h->u3.p) + (size_t)i * d3);
     if (rc) return rc;
+    h->mesh_tw[i] = h->last_trunc;
   }
   return BSMPO_OK;
+}
+
+int bsmpo_mesh_truncation(const bsmpo_ctx* h, double* weights, int cap) {
+  if (!h || (!weights && cap > 0)) return fail(nullptr, BSMPO_EINVAL, "bad argument");
+  const int nb = (int)h->mesh_tw.size();
+  if (!weights) return nb;   // size query
+  if (cap < nb) return fail(const_cast<bsmpo_ctx*>(h), BSMPO_ECAPACITY, "weights buffer too small");
+  std::copy(h->mesh_tw.begin(), h->mesh_tw.end(), weights);
+  return nb;
 }
 
 int bsmpo_apply_phases(bsmpo_ctx* h, const double* phases) {

@@ -162,6 +162,12 @@ cudaError_t launch_contract_sector(int d, int cc0, int cc1, const void* u, const
                                    const void* gcr, const int* cl, const int* cc, const int* cr,
                                    int len_l, int len_c, int len_r, void* c, cudaStream_t s);
 
+// ---------------------------------------------------------------- state.cu
+// Product-state Gamma from the bond charges (sorted, sentinel d) and the per-site
+// density matrices rho[site][o_ket][o_bra] (complex, n d^2 entries).
+cudaError_t launch_product_fill(int n, int d, int chi, const int* charge, const void* rho,
+                                void* gamma, cudaStream_t s);
+
 // ---------------------------------------------------------------- observables.cu
 // env_r[b] (b = n..0) and env_l[b] (b = 0..n), complex, masked to ket == bra charges.
 cudaError_t launch_env_right_step(int d, int chi, const void* gamma_b, const int* charge_b,

@@ -109,24 +109,44 @@ extern "C" int bsmpo_trace_noalloc(int n, int d, int chi, const void* gamma, con
                                      std::to_string(BSMPO_NOALLOC_MAX_CHI));
   if (!gamma || !lambda || !charge || !trace_out)
     return na_fail(BSMPO_EINVAL, "bsmpo_trace_noalloc: null pointer");
+  // an error left by earlier, unrelated work is reported as such, not as ours
+  cudaError_t pe = cudaPeekAtLastError();
+  if (pe != cudaSuccess)
+    return na_fail(BSMPO_ECUDA, std::string("bsmpo_trace_noalloc: pending CUDA error from earlier work: ") +
+                                    cudaGetErrorString(pe));
+  cudaStream_t st = (cudaStream_t)stream;
+  // the scratch address is per device: the stream must belong to the current device
+  int cur = -1, sdev = -1;
+  cudaError_t e = cudaGetDevice(&cur);
+  if (e == cudaSuccess) e = cudaStreamGetDevice(st, &sdev);
+  if (e != cudaSuccess)
+    return na_fail(BSMPO_ECUDA, std::string("bsmpo_trace_noalloc: ") + cudaGetErrorString(e));
+  if (sdev != cur)
+    return na_fail(BSMPO_EINVAL, "bsmpo_trace_noalloc: the stream belongs to device " +
+                                     std::to_string(sdev) + ", the current device is " +
+                                     std::to_string(cur));
   cplx* scratch = nullptr;
   int rc = na_scratch(&scratch);
   if (rc) return rc;
-  cudaStream_t st = (cudaStream_t)stream;
   const cplx* G = reinterpret_cast<const cplx*>(gamma);
   const int2* C = reinterpret_cast<const int2*>(charge);
   const int64_t chi2 = (int64_t)chi * chi;
   cplx* r[2] = {scratch, scratch + chi};
   cplx* part = scratch + 2 * (size_t)BSMPO_NOALLOC_MAX_CHI;
+  auto launched = [](const char* what) -> int {
+    const cudaError_t le = cudaGetLastError();
+    if (le == cudaSuccess) return BSMPO_OK;
+    return na_fail(BSMPO_ECUDA, std::string("bsmpo_trace_noalloc: ") + what + ": " + cudaGetErrorString(le));
+  };
   na_init_kernel<<<ceil_div(chi, 256), 256, 0, st>>>(d, chi, C + (int64_t)n * chi, r[n & 1]);
+  if ((rc = launched("init"))) return rc;
   for (int b = n - 1; b >= 0; --b) {
     // R_b from R_{b+1}; bond b's Lambda is lambda[b-1] for interior bonds
     na_step_kernel<<<ceil_div(chi * 32, 256), 256, 0, st>>>(
         d, chi, G + (int64_t)b * chi2, C + (int64_t)b * chi, b > 0 ? lambda + (int64_t)(b - 1) * chi : nullptr,
         r[(b + 1) & 1], r[b & 1]);
+    if ((rc = launched("environment step"))) return rc;
   }
   na_sum_kernel<<<1, NA_NT, 0, st>>>(chi, r[0], part, trace_out);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return na_fail(BSMPO_ECUDA, std::string("bsmpo_trace_noalloc: ") + cudaGetErrorString(e));
-  return BSMPO_OK;
+  return launched("sum");
 }

@@ -12,49 +12,6 @@ import numpy as np
 from . import _capi
 
 
-def product_state(n_modes, rho_sites, d, chi, total_photons=None):
-    """Product-state MPO with U(1) charges (the reference's ``Initialize`` filling,
-    ``src/MPO.py:56-109``, for arbitrary input modes).
-
-    ``rho_sites[i]`` is mode i's d x d density matrix.  Bond charges are the (ket, bra)
-    photon numbers to the right of the bond, capped at d-1; bond 0 lists every diagonal
-    total (c, c), c < d (or only the post-selected total).  Returns host arrays
-    ``Gamma[n, chi, chi]`` complex128, ``Lambda[n-1, chi]`` float64 (1 on occupied
-    slots) and ``charge[n+1, chi, 2]`` int32 (sentinel d on empty slots).
-    """
-    bonds = [None] * (n_modes + 1)
-    bonds[n_modes] = [(0, 0)]
-    for b in range(n_modes - 1, -1, -1):
-        rho = rho_sites[b]
-        s = set()
-        for (c0, c1) in bonds[b + 1]:
-            for o0 in range(d):
-                for o1 in range(d):
-                    if rho[o0, o1] != 0 and c0 + o0 <= d - 1 and c1 + o1 <= d - 1:
-                        s.add((c0 + o0, c1 + o1))
-        if b == 0:
-            s = {(c, c) for c in range(d)} if total_photons is None else {(total_photons, total_photons)}
-        bonds[b] = sorted(s)
-        if len(bonds[b]) > chi:
-            raise ValueError("chi=%d is smaller than the product-state bond dimension %d" % (chi, len(bonds[b])))
-    gamma = np.zeros((n_modes, chi, chi), dtype=np.complex128)
-    lam = np.zeros((n_modes - 1, chi), dtype=np.float64)
-    charge = np.full((n_modes + 1, chi, 2), d, dtype=np.int32)
-    for b in range(n_modes + 1):
-        for i, c in enumerate(bonds[b]):
-            charge[b, i] = c
-        if 0 < b < n_modes:
-            lam[b - 1, :len(bonds[b])] = 1.0
-    for site in range(n_modes):
-        rho = rho_sites[site]
-        for i, (a0, a1) in enumerate(bonds[site]):
-            for j, (b0, b1) in enumerate(bonds[site + 1]):
-                o0, o1 = a0 - b0, a1 - b1
-                if 0 <= o0 < d and 0 <= o1 < d:
-                    gamma[site, i, j] = rho[o0, o1]
-    return gamma, lam, charge
-
-
 def lossy_single_photon_rhos(n_modes, photon_modes, eta, d):
     """(1-eta)|0><0| + eta|1><1| on ``photon_modes``, vacuum elsewhere."""
     pm = set(int(m) for m in photon_modes)
@@ -167,20 +124,23 @@ class MPOSimulator:
         return g, l, c
 
     def init_product(self, rho_sites, total_photons=None, canonicalize=True):
-        g, l, c = product_state(self.n, rho_sites, self.d, self.chi, total_photons)
-        self.load_host(g, l, c)
+        """Product-state MPO of the per-mode density matrices ``rho_sites`` (n of d x d),
+        built on the device (``bsmpo_init_product``), then canonicalised."""
+        rho = np.ascontiguousarray(np.asarray(rho_sites, dtype=np.complex128))
+        assert rho.shape == (self.n, self.d, self.d)
+        tp = -1 if total_photons is None else int(total_photons)
+        self._chk(self.L.bsmpo_init_product(self.h, _capi.dptr(rho.view(np.float64)), tp))
         if canonicalize:
             self.canonicalize()
 
-    def init_single_photons(self, photon_modes, eta, total_photons=None):
+    def init_single_photons(self, photon_modes, eta, total_photons=None, canonicalize=True):
         """Lossy single photons (transmissivity eta) in ``photon_modes``, canonicalised."""
-        self.init_product(lossy_single_photon_rhos(self.n, photon_modes, eta, self.d), total_photons)
+        self.init_product(lossy_single_photon_rhos(self.n, photon_modes, eta, self.d), total_photons,
+                          canonicalize)
 
     def canonicalize(self):
         """Right-to-left sweep of identity-gate updates (``src/MPO.py:137-155``)."""
-        eye = _m8(np.eye(2))
-        for mode in range(self.n - 2, -1, -1):
-            self._chk(self.L.bsmpo_bs_update(self.h, mode, _capi.dptr(eye)))
+        self._chk(self.L.bsmpo_canonicalize(self.h))
 
     # -------------------------------------------------------------- updates
     def bs_update(self, mode, S):
@@ -200,6 +160,17 @@ class MPOSimulator:
         phi = np.ascontiguousarray(phi, dtype=np.float64)
         self._chk(self.L.bsmpo_run_mesh(self.h, len(modes), _capi.iptr(modes), _capi.dptr(theta),
                                         _capi.dptr(phi)))
+
+    def mesh_truncation(self):
+        """Truncation weight of every update of the last ``run_mesh`` call (mesh order)."""
+        n = self.L.bsmpo_mesh_truncation(self.h, None, 0)
+        if n < 0:
+            _capi.check(n, self.h)
+        out = np.zeros(max(n, 1))
+        n2 = self.L.bsmpo_mesh_truncation(self.h, _capi.dptr(out), len(out))
+        if n2 < 0:
+            _capi.check(n2, self.h)
+        return out[:n]
 
     def apply_phases(self, phases):
         ph = np.ascontiguousarray(phases, dtype=np.float64)

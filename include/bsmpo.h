@@ -94,6 +94,19 @@ int bsmpo_set_cutoff(bsmpo_ctx* h, double cutoff);
 int bsmpo_load_state(bsmpo_ctx* h, const void* gamma, const double* lambda, const int* charge);
 int bsmpo_store_state(bsmpo_ctx* h, void* gamma, double* lambda, int* charge);
 
+/* Product-state MPO built on the device: the filling of the reference's Initialize
+ * (src/MPO.py:56-109) for an arbitrary density matrix per mode.  rho: host
+ * complex128 [n][d][d] (rho[site][ket occupation][bra occupation]).  Bond charges are
+ * the (ket, bra) photons right of the bond, at most d - 1 each; bond 0 lists every
+ * diagonal total (c, c), c < d, or only (total_photons, total_photons) when
+ * total_photons >= 0 (the reference's post-selected photon number).  Lambda = 1 on
+ * occupied slots.  BSMPO_ECAPACITY if a bond needs more than chi slots. */
+int bsmpo_init_product(bsmpo_ctx* h, const double* rho, int total_photons);
+
+/* Right-to-left sweep of identity-gate updates over every bond: the canonicalising
+ * sweep of the reference's Initialize (src/MPO.py:137-155). */
+int bsmpo_canonicalize(bsmpo_ctx* h);
+
 /* Apply a beam splitter to modes (mode, mode+1): the per-BS unit of work of
  * RankWorker.RankProcess (src/beam_splitter_parallel/Rank.py:32-206) and
  * InitializationMPO.Update (src/MPO.py:158-303), fully on the device.
@@ -113,6 +126,13 @@ int bsmpo_bs_update_tensor(bsmpo_ctx* h, int mode, const void* u);
  * same as applying them one by one.  Returns with all work complete. */
 int bsmpo_run_mesh(bsmpo_ctx* h, int n_bs, const int* modes, const double* theta,
                    const double* phi);
+
+/* Truncation weight (sum of discarded sigma^2) of every update of the last
+ * bsmpo_run_mesh call, in mesh order, into host weights[cap].  Returns the number of
+ * updates (>= 0; weights == NULL only queries it) or a negative code
+ * (BSMPO_ECAPACITY if cap is too small).  The
+ * reference computes no truncation weight (src/MPO.py:272-279 discards silently). */
+int bsmpo_mesh_truncation(const bsmpo_ctx* h, double* weights, int cap);
 
 /* Number of updates bsmpo_run_mesh runs at once (1..64, default 8 or the environment
  * variable BSMPO_WORKERS at create).  Each worker owns a stream and its own workspaces
@@ -178,11 +198,17 @@ int bsmpo_stage_times(const bsmpo_ctx* h, double* ms, int n);
  * 2 * BSMPO_NOALLOC_MAX_CHI + 256 complex128 entries (about 135 KB) that every GPU
  * loading the library keeps until the process exits; chi > BSMPO_NOALLOC_MAX_CHI is
  * rejected with BSMPO_EINVAL.  The first call on a device looks up that array's
- * device address (cudaGetSymbolAddress, with the device current), so make the first
- * call on each device before any stream capture.  All calls share the array, and
- * every call rewrites all of the scratch it reads: calls that overlap on the GPU
- * (other streams, other host threads) race; serialise them.  Errors: see
- * bsmpo_last_error(NULL). */
+ * device address (cudaGetSymbolAddress, with the device current) and caches it.  That
+ * first call also makes CUDA load the library's code and the array onto the device
+ * (lazy module loading), which does take device memory once: make the first call on
+ * each device early, before a framework reserves the whole device and before any
+ * stream capture.  The cached address does not survive cudaDeviceReset: do not call
+ * this function again in a process after resetting the device.  `stream` must belong
+ * to the current device on every call (checked: BSMPO_EINVAL otherwise).  A CUDA error
+ * already pending from earlier work makes the call fail with BSMPO_ECUDA before it
+ * launches anything.  All calls share the array, and every call rewrites all of the
+ * scratch it reads: calls that overlap on the GPU (other streams, other host threads)
+ * race; serialise them.  Errors: see bsmpo_last_error(NULL). */
 int bsmpo_trace_noalloc(int n, int d, int chi, const void* gamma, const double* lambda,
                         const int* charge, double* trace_out, void* stream);
 

@@ -158,49 +158,67 @@ def test_single_update_sigma_kept_and_weight(case):
 
 
 # ------------------------------------------------------------------ whole circuits
-def _run_gpu(n, eta, d, chi, seed, phases=True):
+def _run_gpu(n, eta, d, chi, seed, phases=True, max_layers=None):
+    """The mesh (or its first max_layers brick-wall layers) in one run_mesh call."""
     U, bs, ph = interferometer.circuit(n, seed)
+    if max_layers is not None:
+        bs = [b for b in bs if b[0] < max_layers]
     with engine.MPOSimulator(n, d, chi) as sim:
         sim.init_single_photons(range(0, n, 2), eta)
-        layers = {}
-        for (l, m, th, p) in bs:
-            layers.setdefault(l, []).append((m, th, p))
-        for l in sorted(layers):
-            ops = layers[l]
-            sim.run_mesh([o[0] for o in ops], [o[1] for o in ops], [o[2] for o in ops])
+        sim.run_mesh([b[1] for b in bs], [b[2] for b in bs], [b[3] for b in bs])
+        tw = sim.mesh_truncation()
         if phases:
             sim.apply_phases(ph)
         tr, P = sim.observables()
         g, lam, chg = sim.store()
         dims = sim.bond_dims()
-    return tr, P, lam.cpu().numpy(), chg.cpu().numpy(), dims
+    return tr, P, lam.cpu().numpy(), chg.cpu().numpy(), dims, tw
+
+
+def _check_circuit(fx, w, tr, P, lam, chg, dims, tw):
+    """Trace, marginals, per-bond spectra by charge, bond dimensions and per-update
+    truncation weights against an oracle fixture (tolerances of the FP64 path)."""
+    tr_o = complex(fx["trace"][0])
+    assert abs(tr - tr_o) <= TOL * abs(tr_o), (tr, tr_o)
+    np.testing.assert_allclose(P, fx["marginals"], atol=TOL * abs(tr_o))
+    assert dims == [int(x) for x in fx["bond_dims"]]
+    for b in range(1, w["n"]):
+        _close_spectra(_spectra(lam[b - 1], chg[b], w["d"]), _spectra(fx["lam"][b - 1], fx["charge"][b], w["d"]),
+                       TOL * max(1e-300, float(fx["lam"][b - 1].max())))
+    # truncation weight of every update, normwise: |d tw| <= 1e-10 (total sigma^2 of the update)
+    tw_o = fx["trunc_weight"]
+    assert len(tw) == len(tw_o)
+    bad = np.nonzero(np.abs(tw - tw_o) > TOL * fx["total_weight"])[0]
+    assert len(bad) == 0, [(int(i), tw[i], tw_o[i]) for i in bad[:5]]
 
 
 def test_plain_small_circuit_matches_oracle():
     """Workload 1: N=16, 8 photons (even modes), eta=0.5, d=4, chi=64, 120 BSs."""
     fx = np.load(os.path.join(GOLDEN, "oracle_plain_small.npz"))
     w = circuit.WORKLOADS["plain-small"]
-    tr, P, lam, chg, dims = _run_gpu(**w)
-    tr_o = complex(fx["trace"][0])
-    assert abs(tr - tr_o) <= TOL * abs(tr_o), (tr, tr_o)
-    np.testing.assert_allclose(P, fx["marginals"], atol=TOL * abs(tr_o))
-    for b in range(1, w["n"]):
-        _close_spectra(_spectra(lam[b - 1], chg[b], w["d"]), _spectra(fx["lam"][b - 1], fx["charge"][b], w["d"]),
-                       TOL * max(1.0, float(fx["lam"][b - 1].max())))
-    assert dims == [int(x) for x in fx["bond_dims"]]
+    _check_circuit(fx, w, *_run_gpu(**w))
 
 
 def test_plain_scale_circuit_matches_oracle():
     """Workload 2: N=32, 16 photons, eta=0.5, d=4, chi=256, 496 BSs (truncating)."""
-    path = os.path.join(GOLDEN, "oracle_plain_scale.npz")
-    fx = np.load(path)
+    fx = np.load(os.path.join(GOLDEN, "oracle_plain_scale.npz"))
     w = circuit.WORKLOADS["plain-scale"]
-    tr, P, lam, chg, dims = _run_gpu(**w)
-    tr_o = complex(fx["trace"][0])
-    assert abs(tr - tr_o) <= TOL * abs(tr_o), (tr, tr_o)
-    np.testing.assert_allclose(P, fx["marginals"], atol=TOL * abs(tr_o))
+    tr, P, lam, chg, dims, tw = _run_gpu(**w)
+    _check_circuit(fx, w, tr, P, lam, chg, dims, tw)
     # size-independent property: every mode's marginal sums to the trace (positivity is
     # not one: truncating a density-matrix MPO can leave marginals slightly negative)
+    np.testing.assert_allclose(P.sum(axis=1), np.full(w["n"], tr), atol=1e-12 * abs(tr))
+
+
+def test_chi1024_workload_first_layers_match_oracle():
+    """The benchmarked workload (N=64, 32 photons, eta=0.3, d=5, chi=1024, seed 1003):
+    its first 11 brick-wall layers (341 updates; every interior bond saturated at
+    chi = 1024 from layer 5 on) against the oracle's run of the same layers."""
+    fx = np.load(os.path.join(GOLDEN, "oracle_precision_l11.npz"))
+    w = circuit.WORKLOADS["precision"]
+    tr, P, lam, chg, dims, tw = _run_gpu(**w, phases=False, max_layers=11)
+    assert len(tw) == int(fx["n_bs"][0])
+    _check_circuit(fx, w, tr, P, lam, chg, dims, tw)
     np.testing.assert_allclose(P.sum(axis=1), np.full(w["n"], tr), atol=1e-12 * abs(tr))
 
 
@@ -279,6 +297,34 @@ def test_kat_hong_ou_mandel():
     np.testing.assert_allclose(P[0].real, [0.5, 0.0, 0.5], atol=1e-14)
 
 
+# ------------------------------------------------------------------ initial state on the device
+@pytest.mark.parametrize("n,d,chi,tp", [(6, 3, 16, None), (16, 4, 64, None), (9, 5, 32, None), (6, 4, 16, 2)])
+def test_product_state_built_on_device_matches_oracle(n, d, chi, tp):
+    rhos = [mpo.single_photon_rho(d, 0.4) if i % 2 == 0 else mpo.vacuum_rho(d) for i in range(n)]
+    rng = np.random.default_rng(n * d)
+    # one mode with a coherence (off-diagonal) entry, so ket != bra charges occur
+    rhos[1] = rhos[1].copy()
+    rhos[1][0, 1] = rhos[1][1, 0] = 0.1 + 0.05j * rng.standard_normal()
+    rhos[1][1, 0] = np.conj(rhos[1][0, 1])
+    rhos[1][1, 1] = 0.3
+    st = mpo.product_state(n, rhos, d, chi, total_photons=tp)
+    with engine.MPOSimulator(n, d, chi) as sim:
+        sim.init_product(rhos, total_photons=tp, canonicalize=False)
+        g, lam, chg = sim.store()
+        dims = sim.bond_dims()
+    np.testing.assert_array_equal(chg.cpu().numpy(), st.charge)
+    np.testing.assert_array_equal(lam.cpu().numpy(), st.Lambda)
+    np.testing.assert_array_equal(g.cpu().numpy(), st.Gamma)
+    assert dims == mpo.bond_dims(st)
+
+
+def test_init_product_rejects_small_chi():
+    # bond 0 lists the four diagonal totals (c, c), c < 4: three slots are too few
+    with engine.MPOSimulator(8, 4, 3) as sim:
+        with pytest.raises(_capi.BsmpoError, match="smaller than the product-state"):
+            sim.init_single_photons(range(0, 8, 2), 0.5)
+
+
 # ------------------------------------------------------------------ drop-ins and errors
 def test_initialize_dropin_matches_oracle():
     from bosonsampling_b200 import MPO
@@ -314,7 +360,8 @@ def test_errors_are_reported_not_raised_across_the_abi():
     _capi.check(L.bsmpo_create(4, 3, 8, 0, ctypes.byref(h)))
     S = engine._m8(np.eye(2))
     assert L.bsmpo_bs_update(h, 0, _capi.dptr(S)) == -1              # no state loaded
-    g, l, c = engine.product_state(4, engine.lossy_single_photon_rhos(4, [0], 0.5, 3), 3, 8)
+    st = mpo.product_state(4, [mpo.single_photon_rho(3, 0.5)] + [mpo.vacuum_rho(3)] * 3, 3, 8)
+    g, l, c = st.Gamma, st.Lambda, st.charge.copy()
     c[0, [0, 1]] = c[0, [1, 0]]                                        # bond 0 no longer sorted
     gd, ld, cd = (torch.from_numpy(x).cuda() for x in (g, l, c))
     rc = L.bsmpo_load_state(h, ctypes.c_void_p(gd.data_ptr()), ctypes.c_void_p(ld.data_ptr()),

@@ -1,27 +1,15 @@
-"""Host-side logic of the product path, checked on CPU: state builder, mesh
-generator and the 2x2 packing, against the oracle's independent versions."""
+"""Host-side logic of the product path, checked on CPU: the mesh generator and the
+2x2 packing.
+
+The product's Clements decomposition and the oracle's are two copies of one seeded
+algorithm, so their equality below only shows the copies agree; the check of the
+algorithm itself is the reconstruction of U from the mesh and the mesh's shape (the
+single-photon known-answer test on the GPU checks it through the simulation too)."""
 import numpy as np
 import pytest
 
 from bosonsampling_b200 import engine, interferometer
 from oracle import circuit, fock, interferometer as ointerf, mpo
-
-
-@pytest.mark.parametrize("n,d,chi", [(6, 3, 16), (16, 4, 64), (9, 5, 32)])
-def test_product_state_matches_oracle(n, d, chi):
-    rhos = engine.lossy_single_photon_rhos(n, range(0, n, 2), 0.4, d)
-    g, l, c = engine.product_state(n, rhos, d, chi)
-    st = mpo.product_state(n, [mpo.single_photon_rho(d, 0.4) if i % 2 == 0 else mpo.vacuum_rho(d)
-                               for i in range(n)], d, chi)
-    np.testing.assert_array_equal(c, st.charge)
-    np.testing.assert_array_equal(l, st.Lambda)
-    np.testing.assert_allclose(g, st.Gamma)
-
-
-def test_post_selected_bond0():
-    g, l, c = engine.product_state(6, engine.lossy_single_photon_rhos(6, [0, 2, 4], 0.5, 4), 4, 16,
-                                   total_photons=2)
-    assert (c[0, 0] == [2, 2]).all() and (c[0, 1:] == 4).all()
 
 
 @pytest.mark.parametrize("n", [4, 7, 16, 32])
