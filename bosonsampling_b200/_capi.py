@@ -27,6 +27,7 @@ SIGNATURES = {
     "bsmpo_destroy": (_c_int, [_vp]),
     "bsmpo_set_stream": (_c_int, [_vp, _vp]),
     "bsmpo_set_cutoff": (_c_int, [_vp, _c_double]),
+    "bsmpo_set_precision": (_c_int, [_vp, _c_int]),
     "bsmpo_set_workers": (_c_int, [_vp, _c_int]),
     "bsmpo_load_state": (_c_int, [_vp, _vp, _vp, _vp]),
     "bsmpo_store_state": (_c_int, [_vp, _vp, _vp, _vp]),

@@ -72,6 +72,9 @@ struct bsmpo_ctx {
   // workspaces
   DevBuf theta, cbuf, abuf, wbuf, vbuf, sig, keys, perm, tab, tab2, rot, kept, u3, m4, env_l,
       env_r, part, outv, dims, nf2, qbuf, qflag, pbuf, pcnt;
+  // Gram / eigen route of the sector SVD (precision != BSMPO_PRECISION_FP64)
+  DevBuf gbuf, eigd, taub, invsig, escr, swp, zbuf, ybuf;
+  int precision = BSMPO_PRECISION_FP64;
   HostStage stage, stage2, hres;
   // last update diagnostics (host)
   std::vector<int> last_cc, last_shape, last_kept, last_k;
@@ -181,10 +184,13 @@ struct Plan {
   std::vector<SectorDesc> sd;
   std::vector<MixPair> pairs;
   std::vector<GemmGroup> gg;
+  std::vector<GemmGroup> ggram;   // Gram G_s = X^H X of every sector (Gram route)
   std::vector<JacobiWork> jw;
   int mix_tiles = 0, gemm_tiles = 0, max_rounds = 0, max_k = 0, max_left_m2 = 0;
   int gram_ctas = 0, apply_ctas = 0, jac_slots = 0;   // every sector in one round
   int64_t theta_elems = 0, c_elems = 0, a_elems = 0, s_elems = 0, w_elems = 0, v_elems = 0;
+  int64_t g_elems = 0, y_elems = 0;
+  int gram_tiles = 0;
   double flops_theta = 0.0;
 };
 
@@ -234,7 +240,7 @@ int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
   auto rows_of = [&](int a0, int from1) { return T.offL[(a0 + 1) * d] - T.offL[a0 * d + from1]; };
   auto cols_of = [&](int b0, int to1) { return T.offR[b0 * d + to1 + 1] - T.offR[b0 * d]; };
   P.sd.clear();
-  int64_t c_off = 0, a_off = 0, s_off = 0, w_off = 0, v_off = 0;
+  int64_t c_off = 0, a_off = 0, s_off = 0, w_off = 0, v_off = 0, g_off = 0, y_off = 0;
   for (int cc0 = lo0; cc0 <= hi0; ++cc0)
     for (int cc1 = lo1; cc1 <= hi1; ++cc1) {
       SectorDesc S;
@@ -256,6 +262,8 @@ int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
       S.s_off = s_off; s_off += S.k;
       S.w_off = w_off; w_off += (int64_t)S.k * n;
       S.v_off = v_off; v_off += (int64_t)m * S.k;
+      S.g_off = g_off; g_off += (int64_t)S.k * S.k;
+      S.y_off = y_off; y_off += (int64_t)S.k * S.k;
       T.sidx[cc0 * d + cc1] = (int)P.sd.size();
       P.sd.push_back(S);
     }
@@ -267,6 +275,7 @@ int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
   }
   T.n_sectors = ns;
   P.c_elems = c_off; P.a_elems = a_off; P.s_elems = s_off; P.w_elems = w_off; P.v_elems = v_off;
+  P.g_elems = g_off; P.y_elems = y_off;
   // Theta groups (q, a0, b0)
   P.tidx.assign((size_t)dd * d * d, -1);
   P.td.clear();
@@ -314,6 +323,24 @@ int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
     }
   P.theta_elems = t_off;
   P.gemm_tiles = tiles;
+  // Gram groups: G_s = X^H X, X = the first rows_g rows of the sector's Jacobi matrix
+  // ([rows_g][k] row-major: T, or T^H when |L| < |R|)
+  P.ggram.clear();
+  int gtiles = 0;
+  for (const SectorDesc& S : P.sd) {
+    GemmGroup g;
+    std::memset(&g, 0, sizeof(g));
+    g.M = S.k; g.N = S.k; g.K = S.rows_g;
+    g.lda = S.k; g.ldb = S.k; g.ldc = S.k;
+    g.opA = 1; g.opB = 0; g.beta = 0;
+    g.tiles_n = ceil_div(S.k, TNt);
+    g.tile_start = gtiles;
+    gtiles += ceil_div(S.k, TMt) * g.tiles_n;
+    g.a_off = S.a_off; g.b_off = S.a_off; g.c_off = S.g_off;
+    g.ks_off = g.rs_off = g.cs_off = -1;
+    P.ggram.push_back(g);
+  }
+  P.gram_tiles = gtiles;
   T.n_theta = (int)P.td.size();
   // mix pairs (a >= b)
   P.pairs.clear();
@@ -372,7 +399,7 @@ int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
 
 // packs plan tables into the pinned stage and copies them to the device table buffer
 struct TabLayout {
-  size_t tab, tidx, td, sd, pairs, gg, jw, total;
+  size_t tab, tidx, td, sd, pairs, gg, ggram, jw, total;
 };
 
 TabLayout layout_of(const Plan& P) {
@@ -384,6 +411,7 @@ TabLayout layout_of(const Plan& P) {
   L.sd = o; o = align_up(o + P.sd.size() * sizeof(SectorDesc) + 1, 256);
   L.pairs = o; o = align_up(o + P.pairs.size() * sizeof(MixPair) + 1, 256);
   L.gg = o; o = align_up(o + P.gg.size() * sizeof(GemmGroup) + 1, 256);
+  L.ggram = o; o = align_up(o + P.ggram.size() * sizeof(GemmGroup) + 1, 256);
   L.jw = o; o = align_up(o + P.jw.size() * sizeof(JacobiWork) + 1, 256);
   L.total = o;
   return L;
@@ -456,6 +484,7 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   put(hs, L.sd, P.sd);
   put(hs, L.pairs, P.pairs);
   put(hs, L.gg, P.gg);
+  put(hs, L.ggram, P.ggram);
   std::vector<JacobiWork> active(P.jw);
   int gram_ctas = 0, apply_ctas = 0, slots = 0;
   jacobi_launch_list(active, &gram_ctas, &apply_ctas, &slots);
@@ -468,6 +497,8 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   SectorDesc* sd_d = reinterpret_cast<SectorDesc*>(dt + L.sd);
   const MixPair* pairs_d = reinterpret_cast<const MixPair*>(dt + L.pairs);
   const GemmGroup* gg_d = reinterpret_cast<const GemmGroup*>(dt + L.gg);
+  const GemmGroup* ggram_d = reinterpret_cast<const GemmGroup*>(dt + L.ggram);
+  const bool gram = h->precision != BSMPO_PRECISION_FP64;
   const JacobiWork* jw_d = reinterpret_cast<const JacobiWork*>(dt + L.jw);
   const int64_t chi2 = (int64_t)chi * chi;
 
@@ -477,126 +508,153 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
                               P.gemm_tiles, st));
   if ((rc = clk.mark(1))) return rc;
   // 2. identity rows of [T^H; I] and the gate mix
-  CKL(h, launch_identity_rows(sd_d, ns, P.max_left_m2, h->abuf.p, st));
+  if (!gram) CKL(h, launch_identity_rows(sd_d, ns, P.max_left_m2, h->abuf.p, st));
   CKL(h, launch_mix_d(d, tab_d, tidx_d, td_d, sd_d, pairs_d, (int)P.pairs.size(), P.mix_tiles,
                       u3_dev, h->theta.p, h->lam + (size_t)(mode + 2) * chi, h->cbuf.p, h->abuf.p,
                       st));
   if ((rc = clk.mark(2))) return rc;
-  // 3. blocked one-sided Jacobi
-  double* nf2 = reinterpret_cast<double*>(h->nf2.p);
-  CKL(h, launch_sector_norms(sd_d, ns, h->abuf.p, nf2, st));
-  CK(h, cudaMemsetAsync(h->rot.p, 0, (size_t)3 * ns * sizeof(int), st));
-  CK(h, cudaMemsetAsync(h->pcnt.p, 0, std::max(P.jac_slots, 1) * sizeof(int), st));
-  // Convergence polls run one chunk behind: after launching chunk c + 1 the host reads
-  // the counters copied after chunk c, so the stream always has a chunk queued while the
-  // host checks (a converged sector's rounds in the extra chunk exit at once).  Counters
-  // and compacted launch tables alternate between two pinned slots.
-  int* hrot_slot[2] = {reinterpret_cast<int*>(static_cast<char*>(h->hres.p) + 1024), nullptr};
-  hrot_slot[1] = hrot_slot[0] + 3 * ns;
-  const size_t jw_bytes = align_up(std::max<size_t>(P.jw.size(), 1) * sizeof(JacobiWork), 256);
-  if ((rc = grow_host(h, h->stage2, 2 * jw_bytes))) return rc;
-  char* jw_stage[2] = {static_cast<char*>(h->stage2.p), static_cast<char*>(h->stage2.p) + jw_bytes};
-  for (cudaEvent_t& e : h->poll_ev)
-    if (!e) CK(h, cudaEventCreateWithFlags(&e, cudaEventBlockingSync | cudaEventDisableTiming));
-  int t = 0;
-  const int t_max = MAX_SWEEPS * std::max(1, P.max_rounds);
-  bool converged = false;
-  int checks = 0;
-  std::vector<int> conv_at(ns, -1);
-  if (h->timing) CK(h, cudaEventRecord(h->ev0, st));
-  const int chunk = std::max(1, P.max_rounds);   // one sweep of the largest sector
-  int t_after[2] = {0, 0};
-  auto launch_chunk = [&](int slot) -> int {
-    for (int i = 0; i < chunk && t < t_max; ++i, ++t) {
-      // tol <= 0: per-sector default 4 eps sqrt(rows of the Gram), at least 8 eps
-      CK(h, launch_jacobi_round(sd_d, jw_d, (int)active.size(), gram_ctas, apply_ctas, t,
-                                h->abuf.p, reinterpret_cast<int*>(h->rot.p), nf2, 0.0, MAX_SWEEPS,
-                                h->pbuf.p, reinterpret_cast<int*>(h->pcnt.p), h->qbuf.p,
-                                reinterpret_cast<int*>(h->qflag.p), st));
-      h->launches += 2;
+  // 3. the sector SVD: Gram + Hermitian eigenproblem, or blocked one-sided Jacobi
+  double* lam_d = nullptr;
+  double* dbuf_d = nullptr;
+  double* ebuf_d = nullptr;
+  if (gram) {
+    if (P.max_k > eigen_max_k())
+      return fail(h, BSMPO_ECAPACITY, "a sector of dimension " + std::to_string(P.max_k) +
+                                          " exceeds the Gram route's limit " + std::to_string(eigen_max_k()));
+    if ((rc = grow(h, h->gbuf, std::max<int64_t>(P.g_elems, 1) * sizeof(cplx)))) return rc;
+    if ((rc = grow(h, h->eigd, std::max<int64_t>(3 * P.s_elems, 1) * sizeof(double)))) return rc;
+    if ((rc = grow(h, h->taub, std::max<int64_t>(P.s_elems, 1) * sizeof(cplx)))) return rc;
+    if ((rc = grow(h, h->invsig, std::max<int64_t>(P.s_elems, 1) * sizeof(double)))) return rc;
+    dbuf_d = reinterpret_cast<double*>(h->eigd.p);
+    ebuf_d = dbuf_d + P.s_elems;
+    lam_d = ebuf_d + P.s_elems;
+    if (h->timing) CK(h, cudaEventRecord(h->ev0, st));
+    CKL(h, launch_zgemm_grouped(h->abuf.p, h->abuf.p, h->gbuf.p, nullptr, ggram_d, (int)P.ggram.size(),
+                                P.gram_tiles, st));
+    CKL(h, launch_tridiag(sd_d, ns, P.max_k, h->gbuf.p, dbuf_d, ebuf_d, h->taub.p, st));
+    CK(h, launch_bisect(sd_d, ns, P.max_k, dbuf_d, ebuf_d, lam_d, reinterpret_cast<double*>(h->sig.p),
+                        reinterpret_cast<double*>(h->invsig.p), st));
+    h->launches += 2;
+    if (h->timing) CK(h, cudaEventRecord(h->ev1, st));
+    h->last_sweeps = 0;
+    if ((rc = clk.mark(3))) return rc;
+  } else {
+    // 3. blocked one-sided Jacobi
+    double* nf2 = reinterpret_cast<double*>(h->nf2.p);
+    CKL(h, launch_sector_norms(sd_d, ns, h->abuf.p, nf2, st));
+    CK(h, cudaMemsetAsync(h->rot.p, 0, (size_t)3 * ns * sizeof(int), st));
+    CK(h, cudaMemsetAsync(h->pcnt.p, 0, std::max(P.jac_slots, 1) * sizeof(int), st));
+    // Convergence polls run one chunk behind: after launching chunk c + 1 the host reads
+    // the counters copied after chunk c, so the stream always has a chunk queued while the
+    // host checks (a converged sector's rounds in the extra chunk exit at once).  Counters
+    // and compacted launch tables alternate between two pinned slots.
+    int* hrot_slot[2] = {reinterpret_cast<int*>(static_cast<char*>(h->hres.p) + 1024), nullptr};
+    hrot_slot[1] = hrot_slot[0] + 3 * ns;
+    const size_t jw_bytes = align_up(std::max<size_t>(P.jw.size(), 1) * sizeof(JacobiWork), 256);
+    if ((rc = grow_host(h, h->stage2, 2 * jw_bytes))) return rc;
+    char* jw_stage[2] = {static_cast<char*>(h->stage2.p), static_cast<char*>(h->stage2.p) + jw_bytes};
+    for (cudaEvent_t& e : h->poll_ev)
+      if (!e) CK(h, cudaEventCreateWithFlags(&e, cudaEventBlockingSync | cudaEventDisableTiming));
+    int t = 0;
+    const int t_max = MAX_SWEEPS * std::max(1, P.max_rounds);
+    bool converged = false;
+    int checks = 0;
+    std::vector<int> conv_at(ns, -1);
+    if (h->timing) CK(h, cudaEventRecord(h->ev0, st));
+    const int chunk = std::max(1, P.max_rounds);   // one sweep of the largest sector
+    int t_after[2] = {0, 0};
+    auto launch_chunk = [&](int slot) -> int {
+      for (int i = 0; i < chunk && t < t_max; ++i, ++t) {
+        // tol <= 0: per-sector default 4 eps sqrt(rows of the Gram), at least 8 eps
+        CK(h, launch_jacobi_round(sd_d, jw_d, (int)active.size(), gram_ctas, apply_ctas, t,
+                                  h->abuf.p, reinterpret_cast<int*>(h->rot.p), nf2, 0.0, MAX_SWEEPS,
+                                  h->pbuf.p, reinterpret_cast<int*>(h->pcnt.p), h->qbuf.p,
+                                  reinterpret_cast<int*>(h->qflag.p), st));
+        h->launches += 2;
+      }
+      CK(h, cudaMemcpyAsync(hrot_slot[slot], h->rot.p, (size_t)3 * ns * sizeof(int),
+                            cudaMemcpyDeviceToHost, st));
+      CK(h, cudaEventRecord(h->poll_ev[slot], st));
+      t_after[slot] = t;
+      return BSMPO_OK;
+    };
+    if ((rc = launch_chunk(0))) return rc;
+    int cur = 0, compactions = 0;
+    for (;;) {
+      const bool more = t < t_max;
+      if (more && (rc = launch_chunk(cur ^ 1))) return rc;
+      CK(h, cudaEventSynchronize(h->poll_ev[cur]));
+      ++checks;
+      const int* hrot = hrot_slot[cur];
+      bool all = true;
+      for (int s = 0; s < ns; ++s) {
+        // a converged sector leaves the launches, and its counters are stale from then on
+        if (conv_at[s] >= 0) continue;
+        const int R = P.jw[s].rounds;
+        const int done = t_after[cur] / R;
+        if (done < 1 || hrot[3 * s + (done - 1) % 3] != 0) { all = false; continue; }
+        conv_at[s] = done;
+      }
+      if (all) { converged = true; break; }
+      if (!more) break;
+      // drop converged sectors (and those out of sweeps) from the launches after the queued
+      // chunk: the table copy is stream-ordered after it
+      std::vector<JacobiWork> next;
+      for (const auto& w : P.jw)
+        if (conv_at[w.sector] < 0 && t / w.rounds < MAX_SWEEPS) next.push_back(w);
+      if (next.size() < active.size() && !next.empty()) {
+        active.swap(next);
+        jacobi_launch_list(active, &gram_ctas, &apply_ctas, &slots);
+        char* stg = jw_stage[compactions++ & 1];
+        put(stg, 0, active);
+        CK(h, cudaMemcpyAsync(dt + L.jw, stg, active.size() * sizeof(JacobiWork),
+                              cudaMemcpyHostToDevice, st));
+      }
+      cur ^= 1;
     }
-    CK(h, cudaMemcpyAsync(hrot_slot[slot], h->rot.p, (size_t)3 * ns * sizeof(int),
-                          cudaMemcpyDeviceToHost, st));
-    CK(h, cudaEventRecord(h->poll_ev[slot], st));
-    t_after[slot] = t;
-    return BSMPO_OK;
-  };
-  if ((rc = launch_chunk(0))) return rc;
-  int cur = 0, compactions = 0;
-  for (;;) {
-    const bool more = t < t_max;
-    if (more && (rc = launch_chunk(cur ^ 1))) return rc;
-    CK(h, cudaEventSynchronize(h->poll_ev[cur]));
-    ++checks;
-    const int* hrot = hrot_slot[cur];
-    bool all = true;
-    for (int s = 0; s < ns; ++s) {
-      // a converged sector leaves the launches, and its counters are stale from then on
-      if (conv_at[s] >= 0) continue;
-      const int R = P.jw[s].rounds;
-      const int done = t_after[cur] / R;
-      if (done < 1 || hrot[3 * s + (done - 1) % 3] != 0) { all = false; continue; }
-      conv_at[s] = done;
+    if (h->timing) CK(h, cudaEventRecord(h->ev1, st));
+    // sweeps the slowest sector needed (its last one without rotations included); t also
+    // counts the chunk queued after convergence, whose rounds exit at once
+    {
+      int sw = 0;
+      for (int s = 0; s < ns; ++s) sw = std::max(sw, conv_at[s] >= 0 ? conv_at[s] : t / P.jw[s].rounds);
+      h->last_sweeps = sw;
     }
-    if (all) { converged = true; break; }
-    if (!more) break;
-    // drop converged sectors (and those out of sweeps) from the launches after the queued
-    // chunk: the table copy is stream-ordered after it
-    std::vector<JacobiWork> next;
-    for (const auto& w : P.jw)
-      if (conv_at[w.sector] < 0 && t / w.rounds < MAX_SWEEPS) next.push_back(w);
-    if (next.size() < active.size() && !next.empty()) {
-      active.swap(next);
-      jacobi_launch_list(active, &gram_ctas, &apply_ctas, &slots);
-      char* stg = jw_stage[compactions++ & 1];
-      put(stg, 0, active);
-      CK(h, cudaMemcpyAsync(dt + L.jw, stg, active.size() * sizeof(JacobiWork),
-                            cudaMemcpyHostToDevice, st));
+    h->jacobi_rounds += t;   // launched rounds, including the drained chunk
+    if (h->timing) {
+      float ms = 0.f;
+      CK(h, cudaEventSynchronize(h->ev1));
+      CK(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+      h->jac_ms += ms;
+      h->jac_launches += t;
+      // algorithmic flops of the executed sweeps: per block pair and round the pair
+      // Gram (rows_g) and the rotation (rows_tot) of 32 columns, 8 flops per complex MAC
+      for (int s = 0; s < ns; ++s) {
+        const SectorDesc& S = P.sd[s];
+        const double sweeps = conv_at[s] > 0 ? conv_at[s] : (double)t / P.jw[s].rounds;
+        const double cols = 2.0 * jacobi_block_cols();
+        h->jac_flops += sweeps * P.jw[s].rounds * P.jw[s].npairs * 8.0 * cols * cols *
+                        ((double)S.rows_g + S.rows_tot);
+      }
     }
-    cur ^= 1;
+    if ((rc = clk.mark(3))) return rc;
+    if (!converged) {
+      std::string msg = "Jacobi SVD did not converge (mode " + std::to_string(mode) + ")";
+      for (int s = 0; s < ns; ++s) {
+        const int R = P.jw[s].rounds, done = t_after[cur] / R;
+        if (conv_at[s] >= 0) continue;
+        const SectorDesc& S = P.sd[s];
+        msg += "; sector (" + std::to_string(S.cc0) + "," + std::to_string(S.cc1) + ") m=" +
+               std::to_string(S.m) + " n=" + std::to_string(S.n) + " sweeps=" + std::to_string(done) +
+               " rotations=" + std::to_string(hrot_slot[cur][3 * s + (done - 1 + 3) % 3]);
+        break;
+      }
+      return fail(h, BSMPO_ECONVERGE, msg);
+    }
+    CKL(h, launch_jacobi_finish(sd_d, ns, P.max_k, h->abuf.p, nf2,
+                                reinterpret_cast<double*>(h->sig.p),
+                                reinterpret_cast<int*>(h->perm.p), st));
   }
-  if (h->timing) CK(h, cudaEventRecord(h->ev1, st));
-  // sweeps the slowest sector needed (its last one without rotations included); t also
-  // counts the chunk queued after convergence, whose rounds exit at once
-  {
-    int sw = 0;
-    for (int s = 0; s < ns; ++s) sw = std::max(sw, conv_at[s] >= 0 ? conv_at[s] : t / P.jw[s].rounds);
-    h->last_sweeps = sw;
-  }
-  h->jacobi_rounds += t;   // launched rounds, including the drained chunk
-  if (h->timing) {
-    float ms = 0.f;
-    CK(h, cudaEventSynchronize(h->ev1));
-    CK(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-    h->jac_ms += ms;
-    h->jac_launches += t;
-    // algorithmic flops of the executed sweeps: per block pair and round the pair
-    // Gram (rows_g) and the rotation (rows_tot) of 32 columns, 8 flops per complex MAC
-    for (int s = 0; s < ns; ++s) {
-      const SectorDesc& S = P.sd[s];
-      const double sweeps = conv_at[s] > 0 ? conv_at[s] : (double)t / P.jw[s].rounds;
-      const double cols = 2.0 * jacobi_block_cols();
-      h->jac_flops += sweeps * P.jw[s].rounds * P.jw[s].npairs * 8.0 * cols * cols *
-                      ((double)S.rows_g + S.rows_tot);
-    }
-  }
-  if ((rc = clk.mark(3))) return rc;
-  if (!converged) {
-    std::string msg = "Jacobi SVD did not converge (mode " + std::to_string(mode) + ")";
-    for (int s = 0; s < ns; ++s) {
-      const int R = P.jw[s].rounds, done = t_after[cur] / R;
-      if (conv_at[s] >= 0) continue;
-      const SectorDesc& S = P.sd[s];
-      msg += "; sector (" + std::to_string(S.cc0) + "," + std::to_string(S.cc1) + ") m=" +
-             std::to_string(S.m) + " n=" + std::to_string(S.n) + " sweeps=" + std::to_string(done) +
-             " rotations=" + std::to_string(hrot_slot[cur][3 * s + (done - 1 + 3) % 3]);
-      break;
-    }
-    return fail(h, BSMPO_ECONVERGE, msg);
-  }
-  CKL(h, launch_jacobi_finish(sd_d, ns, P.max_k, h->abuf.p, nf2,
-                              reinterpret_cast<double*>(h->sig.p),
-                              reinterpret_cast<int*>(h->perm.p), st));
   // 4. selection -> kept counts (the one host sync of the update)
   int* kept_d = reinterpret_cast<int*>(h->kept.p);
   double* trunc_d = reinterpret_cast<double*>(static_cast<char*>(h->kept.p) +
@@ -610,15 +668,17 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   CK(h, host_wait(h));
   const int total_kept = hk[ns];
   if ((rc = clk.mark(4))) return rc;
-  // 5. V and W = V^H C
-  std::vector<GemmGroup> wg;
-  int wtiles = 0, max_vm = 0;
+  // 5. V (Jacobi: extracted from the converged columns; Gram route: eigenvectors, and
+  // V = T Y diag(1/sigma) where X = T) and W = V^H C
+  std::vector<GemmGroup> wg, vg;
+  int wtiles = 0, vtiles = 0, max_vm = 0, kept_max = 0;
   double flops_w = 0.0;
   const int TMt = zgemm_tile_m(), TNt = zgemm_tile_n();
   for (int s = 0; s < ns; ++s) {
     const SectorDesc& S = P.sd[s];
     const int kp = hk[s];
     max_vm = std::max(max_vm, kp * S.m);
+    kept_max = std::max(kept_max, kp);
     if (kp == 0) continue;
     GemmGroup g;
     std::memset(&g, 0, sizeof(g));
@@ -632,17 +692,51 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
     g.ks_off = g.rs_off = g.cs_off = -1;
     wg.push_back(g);
     flops_w += 8.0 * kp * (double)S.m * S.n;
+    if (gram && !S.left) {
+      // V [m][kp] = T [m][k] Y [k][kp] diag(1 / sigma)
+      GemmGroup v;
+      std::memset(&v, 0, sizeof(v));
+      v.M = S.m; v.N = kp; v.K = S.k;
+      v.lda = S.k; v.ldb = kp; v.ldc = kp;
+      v.opA = 0; v.opB = 0; v.beta = 0;
+      v.tiles_n = ceil_div(kp, TNt);
+      v.tile_start = vtiles;
+      vtiles += ceil_div(S.m, TMt) * v.tiles_n;
+      v.a_off = S.a_off; v.b_off = S.y_off; v.c_off = S.v_off;
+      v.ks_off = v.rs_off = -1;
+      v.cs_off = S.s_off;
+      vg.push_back(v);
+      flops_w += 8.0 * kp * (double)S.m * S.k;
+    }
   }
   const size_t wbytes = align_up(wg.size() * sizeof(GemmGroup) + 1, 256);
-  if ((rc = grow(h, h->tab2, wbytes))) return rc;
-  if ((rc = grow_host(h, h->stage2, wbytes))) return rc;
+  const size_t vbytes = align_up(vg.size() * sizeof(GemmGroup) + 1, 256);
+  if ((rc = grow(h, h->tab2, wbytes + vbytes))) return rc;
+  if ((rc = grow_host(h, h->stage2, wbytes + vbytes))) return rc;
   put(h->stage2.p, 0, wg);
-  CK(h, cudaMemcpyAsync(h->tab2.p, h->stage2.p, wbytes, cudaMemcpyHostToDevice, st));
-  CKL(h, launch_extract_v(sd_d, ns, max_vm, h->abuf.p, reinterpret_cast<double*>(h->sig.p),
-                          reinterpret_cast<int*>(h->perm.p), h->vbuf.p, st));
-  CKL(h, launch_zgemm_grouped(h->vbuf.p, h->cbuf.p, h->wbuf.p, nullptr,
-                              reinterpret_cast<const GemmGroup*>(h->tab2.p), (int)wg.size(), wtiles,
-                              st));
+  put(h->stage2.p, wbytes, vg);
+  CK(h, cudaMemcpyAsync(h->tab2.p, h->stage2.p, wbytes + vbytes, cudaMemcpyHostToDevice, st));
+  const GemmGroup* wg_d = reinterpret_cast<const GemmGroup*>(h->tab2.p);
+  const GemmGroup* vg_d = reinterpret_cast<const GemmGroup*>(static_cast<char*>(h->tab2.p) + wbytes);
+  if (gram) {
+    const size_t ye = (size_t)std::max<int64_t>(P.y_elems, 1);
+    if ((rc = grow(h, h->escr, 4 * ye * sizeof(double)))) return rc;
+    if ((rc = grow(h, h->swp, ye))) return rc;
+    if ((rc = grow(h, h->zbuf, ye * sizeof(double)))) return rc;
+    if ((rc = grow(h, h->ybuf, ye * sizeof(cplx)))) return rc;
+    CK(h, launch_eigvec(sd_d, ns, P.max_k, kept_max, dbuf_d, ebuf_d, lam_d,
+                        reinterpret_cast<double*>(h->escr.p), reinterpret_cast<unsigned char*>(h->swp.p),
+                        reinterpret_cast<double*>(h->zbuf.p), h->gbuf.p, h->taub.p, h->vbuf.p, h->ybuf.p,
+                        st));
+    h->launches += 2;
+    if (!vg.empty())
+      CKL(h, launch_zgemm_grouped(h->abuf.p, h->ybuf.p, h->vbuf.p, reinterpret_cast<double*>(h->invsig.p),
+                                  vg_d, (int)vg.size(), vtiles, st));
+  } else {
+    CKL(h, launch_extract_v(sd_d, ns, max_vm, h->abuf.p, reinterpret_cast<double*>(h->sig.p),
+                            reinterpret_cast<int*>(h->perm.p), h->vbuf.p, st));
+  }
+  CKL(h, launch_zgemm_grouped(h->vbuf.p, h->cbuf.p, h->wbuf.p, nullptr, wg_d, (int)wg.size(), wtiles, st));
   if ((rc = clk.mark(5))) return rc;
   // 6. scatter into Gamma[mode], Gamma[mode+1], Lambda / charge of bond mode+1
   CKL(h, launch_scatter(tab_d, sd_d, ns, total_kept, chi, h->charge + (size_t)mode * chi * 2,
@@ -687,7 +781,6 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   h->last_trunc = *htw;
   h->last_gemm = P.flops_theta + flops_w;
   h->last_svd = svd_flops * h->last_sweeps;
-  (void)checks;
   return BSMPO_OK;
 }
 
@@ -705,7 +798,8 @@ void free_workspaces(bsmpo_ctx* h) {
   DevBuf* bufs[] = {&h->theta, &h->cbuf, &h->abuf, &h->wbuf, &h->vbuf, &h->sig, &h->keys,
                     &h->perm, &h->tab, &h->tab2, &h->rot, &h->kept, &h->u3, &h->m4,
                     &h->env_l, &h->env_r, &h->part, &h->outv, &h->dims, &h->nf2, &h->qbuf,
-                    &h->qflag, &h->pbuf, &h->pcnt};
+                    &h->qflag, &h->pbuf, &h->pcnt, &h->gbuf, &h->eigd, &h->taub, &h->invsig,
+                    &h->escr, &h->swp, &h->zbuf, &h->ybuf};
   for (DevBuf* b : bufs)
     if (b->p) cudaFreeAsync(b->p, h->stream);
   cudaStreamSynchronize(h->stream);
@@ -763,6 +857,7 @@ int run_mesh_concurrent(bsmpo_ctx* h, int n_bs, const int* modes, const cplx* u3
   for (int k = 0; k < nw; ++k) {
     bsmpo_ctx* w = h->workers[k];
     w->cutoff = h->cutoff;
+    w->precision = h->precision;
     w->jac_rows = h->jac_rows;
     w->timing = h->timing;
     if (w->timing && !w->ev0) {
@@ -1009,6 +1104,14 @@ int bsmpo_set_workers(bsmpo_ctx* h, int n_workers) {
 int bsmpo_set_stream(bsmpo_ctx* h, void* stream) {
   if (!h) return fail(nullptr, BSMPO_EINVAL, "null handle");
   h->stream = (cudaStream_t)stream;
+  return BSMPO_OK;
+}
+
+int bsmpo_set_precision(bsmpo_ctx* h, int precision) {
+  if (!h) return fail(nullptr, BSMPO_EINVAL, "null handle");
+  if (precision != BSMPO_PRECISION_FP64 && precision != BSMPO_PRECISION_FP64_GRAM)
+    return fail(h, BSMPO_EINVAL, "unknown precision mode " + std::to_string(precision));
+  h->precision = precision;
   return BSMPO_OK;
 }
 

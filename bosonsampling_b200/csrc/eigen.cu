@@ -1,0 +1,596 @@
+// Gram / Hermitian-eigen route of the per-sector SVD (the mixed-precision form).
+//
+// The reference takes a thin SVD of every sector (cuSOLVER gesvd,
+// src/beam_splitter_parallel/Rank.py:122-125; LAPACK, src/MPO.py:258).  The truncation
+// keeps only the largest chi singular triplets over all sectors (at chi = 1024 about a
+// third of the candidates, cut near 3e-3 of the largest singular value), so this route
+// forms the Gram matrix of each sector in FP64 and solves a Hermitian eigenproblem:
+//   X = T (|L| >= |R|) or T^H (|L| < |R|), G = X^H X (k x k, k = min(|L|, |R|)),
+//   1. Householder reduction of G to a real symmetric tridiagonal (d, e): G = Q T Q^H,
+//      Q = H_0 ... H_{k-2}, H_j = I - tau_j v_j v_j^H (LAPACK's zhetd2 conventions,
+//      lower storage), one thread-block cluster per sector, rows owned cyclically by
+//      the cluster's CTAs, the rank-2 update of step j - 1 fused with the matrix-vector
+//      product of step j (one read and one write of the trailing matrix per step);
+//   2. every eigenvalue by multisection of Sturm counts (one warp per eigenvalue, 32
+//      points per pass), sigma = sqrt(lambda), zero below the numerical floor;
+//   3. after the global top-chi selection: eigenvectors of the kept eigenvalues by
+//      inverse iteration on T - lambda I (partial pivoting; members of tight clusters
+//      of eigenvalues are orthogonalised against each other), then y = Q z.
+// V = y directly when X = T^H (G = T T^H), else V = T Y diag(1/sigma) (a GEMM).
+// Eigenvalue errors are about eps ||G||: singular values above ~1e-6 of the largest
+// are accurate to ~1e-10 relative, far below the truncation cut.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace cg = cooperative_groups;
+
+namespace {
+
+constexpr double EPS = 2.220446049250313e-16;
+constexpr int TD_CL = 8;     // CTAs per sector (one cluster)
+constexpr int TD_NT = 256;
+
+// dynamic shared memory of the tridiagonalisation (kmax = largest k of the launch)
+__host__ __device__ inline size_t td_smem_bytes(int kmax) {
+  const int own = kmax / TD_CL + 1;
+  return sizeof(cplx) * ((size_t)5 * kmax + 2 * (size_t)own) + 64 * sizeof(double);
+}
+
+__device__ __forceinline__ cplx warp_sum(cplx v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+  }
+  return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// a / b for complex b != 0
+__device__ __forceinline__ cplx cdiv(cplx a, cplx b) {
+  const double den = b.x * b.x + b.y * b.y;
+  return cmake((a.x * b.x + a.y * b.y) / den, (a.y * b.x - a.x * b.y) / den);
+}
+
+// ---------------------------------------------------------------------------------
+// 1. Tridiagonalisation.  Cluster c handles sector c; CTA `rank` owns the rows
+//    i = rank (mod TD_CL).  Per step j (trailing size t = k - j - 1):
+//    S0  owner of row j: apply the pending update of step j - 1 to row j, form the
+//        reflector from x = conj(A[j][j+1:]) (zlarfg: beta real), store v_j in row j,
+//        d_j, e_j = beta, tau_j; publish v_j and tau_j in its shared memory;
+//    --  cluster barrier
+//    S1  every CTA: copy v_j; for its rows i > j: A[i][l] -= v'_i conj(w'_l) +
+//        w'_i conj(v'_l) (v', w' of step j - 1), write back, p_i = tau sum_l A[i][l] v_l;
+//        partial c = sum conj(p_i) v_i;
+//    --  cluster barrier
+//    S2  c = sum of the partials; w_i = p_i - tau c / 2 v_i on its rows; publish;
+//    --  cluster barrier
+//    S3  gather the whole w_j (it is v', w' of the next step).
+// Every row is read and written by its owner only, so the trailing matrix needs no
+// ordering across CTAs; the vectors travel through distributed shared memory.
+__global__ void __cluster_dims__(TD_CL, 1, 1) __launch_bounds__(TD_NT)
+    tridiag_kernel(const SectorDesc* __restrict__ sd, int kmax, cplx* __restrict__ gbuf,
+                   double* __restrict__ dbuf, double* __restrict__ ebuf, cplx* __restrict__ taubuf) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int own_cap = kmax / TD_CL + 1;
+  // v and w of two consecutive steps (ping-pong): vb + (j & 1) kmax, wb + (j & 1) kmax
+  cplx* vb = reinterpret_cast<cplx*>(smem_raw);
+  cplx* wb = vb + 2 * kmax;
+  cplx* vpub = wb + 2 * kmax;          // v_j as published by the owner (index l: column j+1+l)
+  cplx* pown = vpub + kmax;            // p_i of the own rows (local index i / TD_CL)
+  cplx* wown = pown + own_cap;         // w_i of the own rows
+  double* scal = reinterpret_cast<double*>(wown + own_cap);   // [0..1] cpart, [2..3] tau, [8..] reduction
+  const SectorDesc& S = sd[blockIdx.x / TD_CL];
+  const int k = S.k;                   // the same for every CTA of the cluster
+  cplx* A = gbuf + S.g_off;
+  double* dd = dbuf + S.s_off;
+  double* ee = ebuf + S.s_off;
+  cplx* tt = taubuf + S.s_off;
+  if (k <= 1) {
+    if (k == 1 && rank == 0 && tid == 0) dd[0] = A[0].x;
+    return;                            // uniform over the cluster
+  }
+  for (int j = 0; j < k - 1; ++j) {
+    const int t = k - j - 1;
+    const int owner = j % TD_CL;
+    cplx* vcur = vb + (j & 1) * kmax;
+    const cplx* vprev = vb + ((j + 1) & 1) * kmax;
+    const cplx* wprev = wb + ((j + 1) & 1) * kmax;
+    // ---- S0: the reflector of row j
+    if (rank == owner) {
+      cplx* row = A + (int64_t)j * k;
+      double part = 0.0;
+      const cplx vj = j > 0 ? vprev[j] : cmake(0.0, 0.0), wj = j > 0 ? wprev[j] : cmake(0.0, 0.0);
+      for (int l = j + tid; l < k; l += TD_NT) {
+        cplx a = ldc(row + l);
+        if (j > 0) a = csub(a, cadd(cmulc(vj, wprev[l]), cmulc(wj, vprev[l])));
+        if (l == j) {
+          if (tid == 0) dd[j] = a.x;
+        } else {
+          const cplx x = cconj(a);
+          vpub[l - j - 1] = x;          // x for now, scaled below
+          if (l > j + 1) part += cabs2(x);
+        }
+      }
+      part = warp_sum(part);
+      if (lane == 0) scal[8 + warp] = part;
+      __syncthreads();
+      double xn2 = 0.0;
+      for (int w = 0; w < TD_NT / 32; ++w) xn2 += scal[8 + w];   // fixed order: every thread alike
+      const cplx alpha = vpub[0];
+      cplx tau, sc;
+      double beta;
+      if (xn2 == 0.0 && alpha.y == 0.0) {
+        tau = cmake(0.0, 0.0);
+        beta = alpha.x;
+        sc = cmake(0.0, 0.0);
+      } else {
+        beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2), alpha.x);
+        tau = cmake((beta - alpha.x) / beta, -alpha.y / beta);
+        sc = cdiv(cmake(1.0, 0.0), cmake(alpha.x - beta, alpha.y));
+      }
+      __syncthreads();                  // alpha read by all before vpub[0] changes
+      for (int l = tid; l < t; l += TD_NT) {
+        const cplx v = l == 0 ? cmake(1.0, 0.0) : cmul(sc, vpub[l]);
+        vpub[l] = v;
+        stc(row + j + 1 + l, v);        // v_j kept in row j for the back-transformation
+      }
+      if (tid == 0) {
+        ee[j] = beta;
+        tt[j] = tau;
+        scal[2] = tau.x;
+        scal[3] = tau.y;
+      }
+    }
+    cluster.sync();
+    // ---- S1: fused update + matrix-vector product on the own rows
+    {
+      const cplx* rv = cluster.map_shared_rank(vpub, owner);
+      const double* rs = cluster.map_shared_rank(scal, owner);
+      for (int l = tid; l < t; l += TD_NT) vcur[j + 1 + l] = rv[l];
+      const cplx tau = cmake(rs[2], rs[3]);
+      __syncthreads();
+      // own rows i > j: first own row, then every TD_CL-th
+      const int i0 = j + 1 + ((rank - (j + 1)) % TD_CL + TD_CL) % TD_CL;
+      double cpx = 0.0, cpy = 0.0;
+      for (int i = i0 + warp * TD_CL; i < k; i += TD_CL * (TD_NT / 32)) {
+        cplx* row = A + (int64_t)i * k;
+        const cplx vi = j > 0 ? vprev[i] : cmake(0.0, 0.0), wi = j > 0 ? wprev[i] : cmake(0.0, 0.0);
+        cplx acc = cmake(0.0, 0.0);
+#pragma unroll 4
+        for (int l = j + 1 + lane; l < k; l += 32) {
+          cplx a = ldc(row + l);
+          if (j > 0) {
+            a = csub(a, cadd(cmulc(vi, wprev[l]), cmulc(wi, vprev[l])));
+            stc(row + l, a);
+          }
+          cfma(acc, a, vcur[l]);
+        }
+        acc = warp_sum(acc);
+        const cplx p = cmul(tau, acc);
+        if (lane == 0) pown[i / TD_CL] = p;
+        // conj(p_i) v_i, summed by lane 0 of each warp in row order
+        const cplx cv = ccmul(p, vcur[i]);
+        cpx += cv.x;
+        cpy += cv.y;
+      }
+      if (lane == 0) {
+        scal[8 + 2 * warp] = cpx;
+        scal[9 + 2 * warp] = cpy;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        double sx = 0.0, sy = 0.0;
+        for (int w = 0; w < TD_NT / 32; ++w) { sx += scal[8 + 2 * w]; sy += scal[9 + 2 * w]; }
+        scal[0] = sx;
+        scal[1] = sy;
+      }
+    }
+    cluster.sync();
+    // ---- S2: w on the own rows
+    {
+      const double* rs = cluster.map_shared_rank(scal, owner);
+      const cplx tau = cmake(rs[2], rs[3]);
+      double cx = 0.0, cy = 0.0;
+      for (int q = 0; q < TD_CL; ++q) {   // fixed order
+        const double* qs = cluster.map_shared_rank(scal, q);
+        cx += qs[0];
+        cy += qs[1];
+      }
+      const cplx a2 = cscale(cmul(tau, cmake(cx, cy)), -0.5);
+      const int i0 = j + 1 + ((rank - (j + 1)) % TD_CL + TD_CL) % TD_CL;
+      for (int i = i0 + tid * TD_CL; i < k; i += TD_CL * TD_NT)
+        wown[i / TD_CL] = cadd(pown[i / TD_CL], cmul(a2, vcur[i]));
+    }
+    cluster.sync();
+    // ---- S3: the whole w_j
+    {
+      cplx* wcur = wb + (j & 1) * kmax;
+      for (int l = j + 1 + tid; l < k; l += TD_NT) {
+        const cplx* rw = cluster.map_shared_rank(wown, l % TD_CL);
+        wcur[l] = rw[l / TD_CL];
+      }
+      __syncthreads();
+    }
+  }
+  // last diagonal entry: the update of step k - 2 on A[k-1][k-1]
+  if (rank == (k - 1) % TD_CL && tid == 0) {
+    const int j = k - 1;
+    const cplx v = vb[((k - 2) & 1) * kmax + j], w = wb[((k - 2) & 1) * kmax + j];
+    const cplx a = csub(ldc(A + (int64_t)j * k + j), cadd(cmulc(v, w), cmulc(w, v)));
+    dd[j] = a.x;
+  }
+  cluster.sync();   // no CTA leaves while another may still read its shared memory
+}
+
+// ---------------------------------------------------------------------------------
+// 2. Eigenvalues: warp i of sector s finds the i-th largest eigenvalue of (d, e) by
+//    multisection: 32 Sturm counts per pass (one per lane), the interval shrinks 33x.
+constexpr int BI_NT = 256;
+
+__device__ __forceinline__ int sturm_count(const double* d, const double* e2, int k, double x,
+                                           double pivmin) {
+  double q = d[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  int c = q < 0.0;
+  for (int i = 1; i < k; ++i) {
+    q = (d[i] - x) - e2[i - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    c += q < 0.0;
+  }
+  return c;
+}
+
+__global__ __launch_bounds__(BI_NT) void bisect_kernel(const SectorDesc* __restrict__ sd,
+                                                       const double* __restrict__ dbuf,
+                                                       const double* __restrict__ ebuf,
+                                                       double* __restrict__ lam) {
+  extern __shared__ double bsm[];
+  const SectorDesc& S = sd[blockIdx.y];
+  const int k = S.k;
+  const int first = blockIdx.x * (BI_NT / 32);
+  if (first >= k) return;             // uniform over the CTA
+  double* d = bsm;
+  double* e2 = bsm + k;
+  __shared__ double red[2][BI_NT / 32];
+  __shared__ double bounds[3];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const double* dg = dbuf + S.s_off;
+  const double* eg = ebuf + S.s_off;
+  double lo = 1e300, hi = -1e300, emax = 0.0;
+  for (int i = tid; i < k; i += BI_NT) {
+    const double di = dg[i];
+    const double ea = i > 0 ? fabs(eg[i - 1]) : 0.0, eb = i < k - 1 ? fabs(eg[i]) : 0.0;
+    d[i] = di;
+    if (i < k - 1) e2[i] = eg[i] * eg[i];
+    lo = fmin(lo, di - ea - eb);
+    hi = fmax(hi, di + ea + eb);
+    emax = fmax(emax, eb * eb);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    emax = fmax(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+  }
+  if (lane == 0) { red[0][warp] = lo; red[1][warp] = hi; }
+  __shared__ double red_e[BI_NT / 32];
+  if (lane == 0) red_e[warp] = emax;
+  __syncthreads();
+  if (tid == 0) {
+    double a = red[0][0], b = red[1][0], c = red_e[0];
+    for (int w = 1; w < BI_NT / 32; ++w) { a = fmin(a, red[0][w]); b = fmax(b, red[1][w]); c = fmax(c, red_e[w]); }
+    // widen by a few ulps of the bound so the extreme eigenvalues stay inside
+    const double span = fmax(fabs(a), fabs(b));
+    bounds[0] = a - 4.0 * EPS * span - 1e-300;
+    bounds[1] = b + 4.0 * EPS * span + 1e-300;
+    bounds[2] = 2.2250738585072014e-308 * fmax(1.0, c);   // pivmin
+  }
+  __syncthreads();
+  const int i = first + warp;
+  if (i >= k) return;
+  const int target = k - 1 - i;        // eigenvalues below lambda_(i) (ascending index)
+  const double pivmin = bounds[2];
+  double a = bounds[0], b = bounds[1];
+  for (int it = 0; it < 16; ++it) {
+    const double x = a + (double)(lane + 1) * ((b - a) / 33.0);
+    const int c = sturm_count(d, e2, k, x, pivmin);
+    const unsigned below = __ballot_sync(0xffffffffu, c <= target);
+    const int L = __popc(below);       // counts rise with x: lanes 0..L-1 lie below
+    const double xl = __shfl_sync(0xffffffffu, x, L > 0 ? L - 1 : 0);
+    const double xh = __shfl_sync(0xffffffffu, x, L < 32 ? L : 31);
+    const double na = L > 0 ? xl : a, nb = L < 32 ? xh : b;
+    a = na;
+    b = nb;
+    if (b - a <= 2.0 * EPS * fmax(fabs(a), fabs(b)) + pivmin) break;   // warp-uniform
+  }
+  if (lane == 0) lam[S.s_off + i] = 0.5 * (a + b);
+}
+
+// Monotone order (bisection rounds independently), numerical floor, sigma and 1/sigma.
+constexpr int FI_NT = 1024;
+__global__ __launch_bounds__(FI_NT) void eig_finish_kernel(const SectorDesc* __restrict__ sd,
+                                                           const double* __restrict__ lam,
+                                                           double* __restrict__ sig,
+                                                           double* __restrict__ invsig) {
+  __shared__ double buf[2][FI_NT];
+  const SectorDesc& S = sd[blockIdx.x];
+  const int k = S.k;
+  const int tid = threadIdx.x;
+  // k <= FI_NT * 2 handled in two halves of the scan
+  const double lmax = k > 0 ? lam[S.s_off] : 0.0;
+  const double floor_l = 32.0 * EPS * (double)k * fabs(lmax);
+  double carry = 1e300;
+  for (int base = 0; base < k; base += FI_NT) {
+    const int i = base + tid;
+    double v = i < k ? lam[S.s_off + i] : 1e300;
+    int cur = 0;
+    buf[0][tid] = v;
+    __syncthreads();
+    for (int off = 1; off < FI_NT; off <<= 1) {   // inclusive prefix minimum
+      const double x = buf[cur][tid];
+      const double y = tid >= off ? buf[cur][tid - off] : 1e300;
+      buf[cur ^ 1][tid] = fmin(x, y);
+      cur ^= 1;
+      __syncthreads();
+    }
+    v = fmin(buf[cur][tid], carry);
+    if (i < k) {
+      const double s = v > floor_l ? sqrt(v) : 0.0;
+      sig[S.s_off + i] = s;
+      invsig[S.s_off + i] = s > 0.0 ? 1.0 / s : 0.0;
+    }
+    carry = fmin(carry, buf[cur][FI_NT - 1]);
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// 3a. Eigenvectors of the tridiagonal by inverse iteration, one thread per kept
+//     eigenvalue.  T - lambda I = P L U with partial pivoting (U has two
+//     superdiagonals), stored column-interleaved in the scratch (entry l of vector t
+//     at l * kept + t, so a warp's accesses coalesce).  Start vector: a fixed
+//     pseudo-random one; three solves, normalised.  Eigenvalues closer than `gaptol`
+//     form a group handled by its first member, each vector orthogonalised against
+//     the group's earlier ones after every solve.
+constexpr int IV_NT = 128;
+
+__device__ __forceinline__ double start_entry(int l, int t) {
+  unsigned h = (unsigned)l * 2654435761u ^ ((unsigned)t * 40503u + 0x9e3779b9u);
+  h ^= h >> 15;
+  h *= 2246822519u;
+  h ^= h >> 13;
+  return ((double)(h & 0xffffu) + 0.5) / 32768.0 - 1.0;
+}
+
+__global__ __launch_bounds__(IV_NT) void invit_kernel(const SectorDesc* __restrict__ sd,
+                                                      const double* __restrict__ dbuf,
+                                                      const double* __restrict__ ebuf,
+                                                      const double* __restrict__ lam,
+                                                      double* __restrict__ scratch,
+                                                      unsigned char* __restrict__ swp,
+                                                      double* __restrict__ zbuf) {
+  extern __shared__ double ism[];
+  const SectorDesc& S = sd[blockIdx.y];
+  const int k = S.k, kept = S.kept;
+  const int t0 = blockIdx.x * IV_NT;
+  if (t0 >= kept) return;
+  double* d = ism;
+  double* e = ism + k;
+  for (int i = threadIdx.x; i < k; i += IV_NT) {
+    d[i] = dbuf[S.s_off + i];
+    e[i] = i < k - 1 ? ebuf[S.s_off + i] : 0.0;
+  }
+  __syncthreads();
+  const int t = t0 + threadIdx.x;
+  if (t >= kept) return;
+  const double* lv = lam + S.s_off;
+  const double norm = fmax(fabs(lv[0]), fabs(lv[k - 1]));
+  const double gaptol = 1e-9 * norm;
+  // group membership: not a leader if the previous kept eigenvalue is within gaptol
+  if (t > 0 && lv[t - 1] - lv[t] <= gaptol) return;
+  int g_end = t + 1;
+  while (g_end < kept && lv[g_end - 1] - lv[g_end] <= gaptol) ++g_end;
+  const double tiny = EPS * norm + 1e-300;
+  // scratch layout of this sector: 4 arrays [k][kept] (u0, u1, u2, mult)
+  double* U0 = scratch + 4 * S.y_off;   // 4 arrays of k x kept in the sector's 4 k^2 slots
+  double* U1 = U0 + (int64_t)k * kept;
+  double* U2 = U1 + (int64_t)k * kept;
+  double* MU = U2 + (int64_t)k * kept;
+  unsigned char* SW = swp + S.y_off;
+  double* Z = zbuf + S.y_off;
+  for (int m = t; m < g_end; ++m) {
+    const double lambda = lv[m];
+    // factor T - lambda I
+    double p = d[0] - lambda, q = k > 1 ? e[0] : 0.0;
+    for (int i = 0; i < k - 1; ++i) {
+      const double ei = e[i], an = d[i + 1] - lambda, en = i + 1 < k - 1 ? e[i + 1] : 0.0;
+      const int64_t o = (int64_t)i * kept + m;
+      if (fabs(ei) > fabs(p)) {
+        const double mu = p / ei;
+        U0[o] = ei; U1[o] = an; U2[o] = en; MU[o] = mu; SW[o] = 1;
+        const double np = q - mu * an, nq = -mu * en;
+        p = np;
+        q = nq;
+      } else {
+        if (p == 0.0) p = tiny;
+        const double mu = ei / p;
+        U0[o] = p; U1[o] = q; U2[o] = 0.0; MU[o] = mu; SW[o] = 0;
+        p = an - mu * q;
+        q = en;
+      }
+    }
+    if (p == 0.0) p = tiny;
+    {
+      const int64_t o = (int64_t)(k - 1) * kept + m;
+      U0[o] = p; U1[o] = 0.0; U2[o] = 0.0; MU[o] = 0.0; SW[o] = 0;
+    }
+    for (int it = 0; it < 3; ++it) {
+      // right-hand side: start vector, or L^{-1} P z
+      if (it == 0) {
+        for (int i = 0; i < k; ++i) Z[(int64_t)i * kept + m] = start_entry(i, m);
+      } else {
+        for (int i = 0; i < k - 1; ++i) {
+          const int64_t o = (int64_t)i * kept + m, o1 = o + kept;
+          double bi = Z[o], bn = Z[o1];
+          if (SW[o]) { const double x = bi; bi = bn; bn = x; }
+          Z[o] = bi;
+          Z[o1] = bn - MU[o] * bi;
+        }
+      }
+      // back substitution U z = b, then normalise
+      double z1 = 0.0, z2 = 0.0, nrm = 0.0;
+      for (int i = k - 1; i >= 0; --i) {
+        const int64_t o = (int64_t)i * kept + m;
+        double u0 = U0[o];
+        if (u0 == 0.0) u0 = tiny;
+        const double z = (Z[o] - U1[o] * z1 - U2[o] * z2) / u0;
+        Z[o] = z;
+        z2 = z1;
+        z1 = z;
+        nrm += z * z;
+      }
+      // orthogonalise against the group's earlier vectors
+      for (int g = t; g < m; ++g) {
+        double dot = 0.0;
+        for (int i = 0; i < k; ++i) dot += Z[(int64_t)i * kept + g] * Z[(int64_t)i * kept + m];
+        nrm = 0.0;
+        for (int i = 0; i < k; ++i) {
+          const double z = Z[(int64_t)i * kept + m] - dot * Z[(int64_t)i * kept + g];
+          Z[(int64_t)i * kept + m] = z;
+          nrm += z * z;
+        }
+      }
+      const double inv = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
+      for (int i = 0; i < k; ++i) Z[(int64_t)i * kept + m] *= inv;
+    }
+  }
+}
+
+// 3b. y = Q z = H_0 (H_1 (... H_{k-2} z)), one warp per kept vector; lane holds the
+//     entries l = lane (mod 32).  Writes V = y ([k][kept], X = T^H) or Y for the GEMM.
+constexpr int BT_NT = 256;
+
+template <int NPL>
+__global__ __launch_bounds__(BT_NT) void backtransform_kernel(const SectorDesc* __restrict__ sd,
+                                                              const cplx* __restrict__ gbuf,
+                                                              const cplx* __restrict__ taubuf,
+                                                              const double* __restrict__ zbuf,
+                                                              cplx* __restrict__ vbuf,
+                                                              cplx* __restrict__ ybuf) {
+  const SectorDesc& S = sd[blockIdx.y];
+  const int k = S.k, kept = S.kept;
+  const int lane = threadIdx.x & 31;
+  const int t = blockIdx.x * (BT_NT / 32) + (threadIdx.x >> 5);
+  if (t >= kept) return;
+  const cplx* A = gbuf + S.g_off;
+  const cplx* tau = taubuf + S.s_off;
+  const double* Z = zbuf + S.y_off;
+  cplx y[NPL];
+#pragma unroll
+  for (int c = 0; c < NPL; ++c) {
+    const int l = lane + 32 * c;
+    y[c] = l < k ? cmake(Z[(int64_t)l * kept + t], 0.0) : cmake(0.0, 0.0);
+  }
+  for (int j = k - 2; j >= 0; --j) {
+    const cplx* v = A + (int64_t)j * k;     // v_j at columns j+1 .. k-1 (v[j+1] = 1)
+    cplx dot = cmake(0.0, 0.0);
+#pragma unroll
+    for (int c = 0; c < NPL; ++c) {
+      const int l = lane + 32 * c;
+      if (l > j && l < k) ccfma(dot, ldc(v + l), y[c]);
+    }
+    dot = warp_sum(dot);
+    const cplx f = cmul(tau[j], dot);
+#pragma unroll
+    for (int c = 0; c < NPL; ++c) {
+      const int l = lane + 32 * c;
+      if (l > j && l < k) y[c] = csub(y[c], cmul(f, ldc(v + l)));
+    }
+  }
+  cplx* out = S.left ? vbuf + S.v_off : ybuf + S.y_off;
+#pragma unroll
+  for (int c = 0; c < NPL; ++c) {
+    const int l = lane + 32 * c;
+    if (l < k) stc(out + (int64_t)l * kept + t, y[c]);
+  }
+}
+
+}  // namespace
+
+int eigen_max_k() {
+  // shared memory of the tridiagonalisation: (5 k + 2 (k / 8 + 1)) x 16 B <= 227 KB
+  int k = 256;
+  while (td_smem_bytes(k + 256) <= 227 * 1024) k += 256;
+  return std::min(k, 32 * 32);   // the back-transformation keeps 32 entries per lane
+}
+
+cudaError_t launch_tridiag(const SectorDesc* sd_dev, int n_sectors, int kmax, void* gbuf,
+                           double* dbuf, double* ebuf, void* taubuf, cudaStream_t s) {
+  if (n_sectors <= 0) return cudaSuccess;
+  const size_t smem = td_smem_bytes(kmax);
+  // once per process: the largest dynamic shared memory any launch may ask for
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)td_smem_bytes(eigen_max_k()));
+  if (attr != cudaSuccess) return attr;
+  tridiag_kernel<<<n_sectors * TD_CL, TD_NT, smem, s>>>(sd_dev, kmax, reinterpret_cast<cplx*>(gbuf),
+                                                        dbuf, ebuf, reinterpret_cast<cplx*>(taubuf));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bisect(const SectorDesc* sd_dev, int n_sectors, int kmax, const double* dbuf,
+                          const double* ebuf, double* lam, double* sig, double* invsig,
+                          cudaStream_t s) {
+  if (n_sectors <= 0 || kmax <= 0) return cudaSuccess;
+  const size_t smem = (size_t)2 * kmax * sizeof(double);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  dim3 grid(ceil_div(kmax, BI_NT / 32), n_sectors);
+  bisect_kernel<<<grid, BI_NT, smem, s>>>(sd_dev, dbuf, ebuf, lam);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  eig_finish_kernel<<<n_sectors, FI_NT, 0, s>>>(sd_dev, lam, sig, invsig);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_eigvec(const SectorDesc* sd_dev, int n_sectors, int kmax, int kept_max,
+                          const double* dbuf, const double* ebuf, const double* lam,
+                          double* scratch, unsigned char* swp, double* zbuf, const void* gbuf,
+                          const void* taubuf, void* vbuf, void* ybuf, cudaStream_t s) {
+  if (n_sectors <= 0 || kept_max <= 0) return cudaSuccess;
+  const size_t smem = (size_t)2 * kmax * sizeof(double);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(invit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  invit_kernel<<<dim3(ceil_div(kept_max, IV_NT), n_sectors), IV_NT, smem, s>>>(sd_dev, dbuf, ebuf, lam,
+                                                                               scratch, swp, zbuf);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  dim3 grid(ceil_div(kept_max, BT_NT / 32), n_sectors);
+  const cplx* G = reinterpret_cast<const cplx*>(gbuf);
+  const cplx* T = reinterpret_cast<const cplx*>(taubuf);
+  cplx* V = reinterpret_cast<cplx*>(vbuf);
+  cplx* Y = reinterpret_cast<cplx*>(ybuf);
+  const int npl = ceil_div(kmax, 32);
+  if (npl <= 4) backtransform_kernel<4><<<grid, BT_NT, 0, s>>>(sd_dev, G, T, zbuf, V, Y);
+  else if (npl <= 8) backtransform_kernel<8><<<grid, BT_NT, 0, s>>>(sd_dev, G, T, zbuf, V, Y);
+  else if (npl <= 16) backtransform_kernel<16><<<grid, BT_NT, 0, s>>>(sd_dev, G, T, zbuf, V, Y);
+  else if (npl <= 32) backtransform_kernel<32><<<grid, BT_NT, 0, s>>>(sd_dev, G, T, zbuf, V, Y);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}

@@ -68,7 +68,9 @@ struct SectorDesc {
   int64_t a_off;       // Jacobi matrix, row-major [rows_tot][k] (complex)
   int64_t s_off;       // singular values / keys / permutation (k entries)
   int64_t w_off;       // W = V^H C, [kept][n] row-major (complex)
-  int64_t v_off;       // conj(V) rows, [kept][m] row-major (complex)
+  int64_t v_off;       // V, [m][kept] row-major (complex)
+  int64_t g_off;       // Gram / Householder vectors, [k][k] (complex; Gram route only)
+  int64_t y_off;       // k x k slots (Gram route): eigenvectors [k][kept], scratch
   int row_start[BSMPO_MAX_D];   // row of L_s where left group a0 (a1 >= cc1 part) starts
   int col_start[BSMPO_MAX_D];   // column of R_s where right group b0 (b1 <= cc1 part) starts
 };
@@ -155,6 +157,23 @@ cudaError_t launch_sector_norms(const SectorDesc* sd_dev, int n_sectors, const v
 cudaError_t launch_jacobi_finish(const SectorDesc* sd_dev, int n_sectors, int max_k,
                                  const void* abuf, const double* nf2, double* sig, int* perm,
                                  cudaStream_t s);
+
+// ---------------------------------------------------------------- eigen.cu
+// Gram / Hermitian-eigen route of the sector SVD (see eigen.cu).  gbuf holds every
+// sector's Gram G = X^H X (k x k at g_off), overwritten by the Householder vectors.
+int eigen_max_k();
+cudaError_t launch_tridiag(const SectorDesc* sd_dev, int n_sectors, int kmax, void* gbuf,
+                           double* dbuf, double* ebuf, void* taubuf, cudaStream_t s);
+// eigenvalues (lam, descending), singular values sig = sqrt(lam) (0 below the floor), 1/sig
+cudaError_t launch_bisect(const SectorDesc* sd_dev, int n_sectors, int kmax, const double* dbuf,
+                          const double* ebuf, double* lam, double* sig, double* invsig,
+                          cudaStream_t s);
+// eigenvectors of the kept eigenvalues (sd[s].kept): V ([k][kept] at v_off) of the
+// sectors with X = T^H, Y ([k][kept] at y_off) of the others
+cudaError_t launch_eigvec(const SectorDesc* sd_dev, int n_sectors, int kmax, int kept_max,
+                          const double* dbuf, const double* ebuf, const double* lam,
+                          double* scratch, unsigned char* swp, double* zbuf, const void* gbuf,
+                          const void* taubuf, void* vbuf, void* ybuf, cudaStream_t s);
 
 // ---------------------------------------------------------------- contract.cu
 // Standalone sector contraction with per-element charges (the update_MPO drop-in).

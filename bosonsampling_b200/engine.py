@@ -68,6 +68,13 @@ class MPOSimulator:
     def set_cutoff(self, cutoff):
         self._chk(self.L.bsmpo_set_cutoff(self.h, float(cutoff)))
 
+    PRECISIONS = {"fp64": 0, "fp64-gram": 1}
+
+    def set_precision(self, precision):
+        """Sector SVD / contraction mode: 'fp64' (Jacobi, the plain path) or 'fp64-gram'
+        (FP64 Gram + Hermitian eigenproblem)."""
+        self._chk(self.L.bsmpo_set_precision(self.h, self.PRECISIONS[precision]))
+
     def set_workers(self, n_workers):
         """Beam splitters of one brick-wall layer that ``run_mesh`` runs at once."""
         self._chk(self.L.bsmpo_set_workers(self.h, int(n_workers)))

@@ -83,6 +83,18 @@ int bsmpo_destroy(bsmpo_ctx* h);
 /* Stream used by all following calls on h (default: the legacy default stream). */
 int bsmpo_set_stream(bsmpo_ctx* h, void* stream);
 
+/* How the sector SVD and the contractions are computed (bsmpo_set_precision):
+ *   BSMPO_PRECISION_FP64       one-sided Jacobi SVD in FP64, FP64 contractions: the
+ *                              plain path, equal to the reference CPU algorithm
+ *                              (src/MPO.py:254-279) to ~1e-12 (the default);
+ *   BSMPO_PRECISION_FP64_GRAM  FP64 contractions, per-sector Gram matrix and Hermitian
+ *                              eigenproblem in FP64 (Householder tridiagonalisation,
+ *                              bisection, inverse iteration): singular values below
+ *                              about 2e-6 of the largest are dropped as zero. */
+#define BSMPO_PRECISION_FP64 0
+#define BSMPO_PRECISION_FP64_GRAM 1
+int bsmpo_set_precision(bsmpo_ctx* h, int precision);
+
 /* Relative singular-value cutoff: a singular value s is kept only if
  * s > cutoff * (largest singular value of that update).  0 (the default) keeps every
  * s > 0, the reference's rule (src/MPO.py:272-279 with the Lambda > 0 masks). */
