@@ -41,7 +41,11 @@ WORKLOADS = {
                    n=32, eta=0.5, d=4, chi=256, seed=1002),
 }
 WORKLOAD = WORKLOADS["chi1024"]
-METRIC = "BS-updates/s (chi=1024 circuit, plain FP64 path)"
+METRIC = "BS-updates/s & circuit time at \u03c7=1024 vs plain FP64 GPU path at \u22641e-6 prob err"
+# arithmetic type of each path
+DTYPES = {"fp64": "f64", "fp64-gram": "f64"}
+SVD_KERNELS = {"fp64": "jacobi_gram_kernel + jacobi_apply_kernel (one-sided Jacobi SVD rounds)",
+               "fp64-gram": "zgemm_grouped_kernel (Gram) + tridiag_kernel + bisect_kernel (Gram route SVD)"}
 
 
 def parse():
@@ -56,6 +60,12 @@ def parse():
     p.add_argument("--no-circuit", action="store_true",
                    help="skip the whole-circuit run (all updates from the initial state)")
     p.add_argument("--workload", default="chi1024", choices=sorted(WORKLOADS))
+    p.add_argument("--precision", default="fp64-gram", choices=sorted(DTYPES),
+                   help="the measured path: fp64-gram (Gram matrix + Hermitian eigenproblem, the "
+                        "default) or fp64 (the plain path: one-sided Jacobi)")
+    p.add_argument("--workers", type=int, default=0, help="concurrent updates (0: 16, or 8 for fp64)")
+    p.add_argument("--no-plain", action="store_true",
+                   help="skip the plain FP64 path (the metric's denominator) and the error against it")
     p.add_argument("--bs-slice", default=None,
                    help="profiling runs only: START:STOP -- a step runs beam splitters START..STOP-1 "
                         "of its layer (default: the whole layer)")
@@ -67,8 +77,16 @@ def parse():
     global WORKLOAD, METRIC
     WORKLOAD = WORKLOADS[a.workload]
     if a.workload != "chi1024":
-        METRIC = "BS-updates/s (%s circuit, plain FP64 path)" % a.workload
+        METRIC = "BS-updates/s (%s circuit) vs plain FP64 GPU path" % a.workload
     return a
+
+
+def config_dict(args, workers):
+    """The workload and how a step is timed (the same dict on both arms)."""
+    return {"workload": WORKLOAD["name"],
+            "start_layer": args.start_layer,
+            "l2": "inputs larger than L2 (state 1.07 GB)" if WORKLOAD["chi"] >= 1024 else "state below L2 size",
+            "bs_slice": args.bs_slice or "whole layer", "cutoff": 0.0}
 
 
 def dist_env():
@@ -275,8 +293,10 @@ def run_reference(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": w["name"], "path": "CPU restatement of the reference update (oracle/)",
-                       "step": "bounded sample of the circuit's BS updates from layer %d on" % args.start_layer},
+            "config": config_dict(args, 0),
+            "path": "CPU restatement of the reference update (oracle/), FP64, all BLAS threads",
+            "step": "a bounded sample of the circuit's BS updates from layer %d on (one CPU layer takes "
+                    "~15 s)" % args.start_layer,
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "BS-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -304,22 +324,25 @@ def main():
     need = args.start_layer + args.warmup + args.steps
     if need > len(layers):
         raise SystemExit("start-layer + warmup + steps exceeds the %d layers" % len(layers))
+    workers = args.workers or (8 if args.precision == "fp64" else 16)
     sim = engine.MPOSimulator(w["n"], w["d"], w["chi"])
+    sim.set_workers(workers)
     sim.init_single_photons(range(0, w["n"], 2), w["eta"])
 
     bs_slice = slice(*[int(x) for x in args.bs_slice.split(":")]) if args.bs_slice else slice(None)
 
-    def run_layers(L0, count, partial=False):
+    def layer_ops(L0, count, partial=False):
+        return [op for L in range(L0, L0 + count) for op in (layers[L][bs_slice] if partial else layers[L])]
+
+    def run_layers(h, L0, count, partial=False):
         # one library call for `count` consecutive layers, as a whole-circuit run makes it
         # (the library overlaps consecutive layers' independent updates)
-        ops = [op for L in range(L0, L0 + count) for op in (layers[L][bs_slice] if partial else layers[L])]
+        ops = layer_ops(L0, count, partial)
         if ops:
-            sim.run_mesh([m for (m, _, _) in ops], [t for (_, t, _) in ops], [p for (_, _, p) in ops])
+            h.run_mesh([m for (m, _, _) in ops], [t for (_, t, _) in ops], [p for (_, _, p) in ops])
 
-    def run_layer(L, partial=False):
-        run_layers(L, 1, partial)
-
-    # untimed: advance to the saturated middle of the circuit
+    # untimed: advance to the saturated middle of the circuit on the plain FP64 path, so
+    # both paths time the same layers from the same state
     t_setup = time.perf_counter()
     cache = args.state_cache
     if cache and os.path.exists(cache):
@@ -329,7 +352,7 @@ def main():
         sim.load(saved["gamma"].cuda(), saved["lam"].cuda(), saved["charge"].cuda())
         del saved
     else:
-        run_layers(0, args.start_layer)
+        run_layers(sim, 0, args.start_layer)
         if cache:
             g, l, c = sim.store()
             torch.save({"workload": w["name"], "start_layer": args.start_layer,
@@ -337,133 +360,166 @@ def main():
     torch.cuda.synchronize()
     t_setup = time.perf_counter() - t_setup
     dims = sim.bond_dims()
-    g0, l0, c0 = sim.store()   # the timed layers restart from this state (device copy)
-    g_host = g0.cpu().pin_memory()
-    l_host = l0.cpu().pin_memory()
-    c_host = c0.cpu().pin_memory()
+    g0, l0, c0 = sim.store()          # state at --start-layer (device copy)
 
-    run_layers(args.start_layer, args.warmup)
-    torch.cuda.synchronize()
-
-    # ---- timed, device-resident: K layers after the warm-up ones
     first = args.start_layer + args.warmup
-    n_bs = sum(len(layers[first + i][bs_slice]) for i in range(args.steps))
-    sampler = ClockSampler(local)
-    sim.set_timing(True)
-    launches0 = sim.kernel_launches()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    sampler.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.nvtx.range_push("timed")
-    e0.record()
-    run_layers(first, args.steps, partial=True)
-    e1.record()
-    torch.cuda.synchronize()
-    torch.cuda.nvtx.range_pop()
-    sampler.stop()
-    launches = sim.kernel_launches() - launches0
-    jac_ms, jac_flops, jac_launches = sim.jacobi_timing()
-    sim.set_timing(False)
-    t_dev = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, "cuda")
-    if world > 1:
-        dist.barrier()
-    value = replica_rate(n_bs, world, t_dev)
+    n_bs = len(layer_ops(first, args.steps, partial=True))
 
-    # ---- end to end through the public API with host buffers: per step the state is
-    # copied host -> device and loaded, the layer runs, the state is stored and copied
-    # device -> host, and the trace is read back
-    e2e_steps = 1
-    g_dev = torch.empty_like(g0)
-    l_dev = torch.empty_like(l0)
-    c_dev = torch.empty_like(c0)
-    g_out = torch.empty_like(g_host, pin_memory=True)
+    def timed_layers(precision, n_workers):
+        """W warm-up layers then K timed layers from the start state; device seconds."""
+        sim.load(g0, l0, c0)
+        sim.set_precision(precision)
+        sim.set_workers(n_workers)
+        run_layers(sim, args.start_layer, args.warmup)
+        torch.cuda.synchronize()
+        sim.set_timing(True)
+        launches0 = sim.kernel_launches()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local)
+        sampler.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push("timed")
+        e0.record()
+        run_layers(sim, first, args.steps, partial=True)
+        e1.record()
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        sampler.stop()
+        launches = sim.kernel_launches() - launches0
+        svd_ms, svd_flops, svd_launches = sim.jacobi_timing()
+        sim.set_timing(False)
+        t = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, "cuda")
+        tr, P = sim.observables()
+        return {"seconds": t, "launches": launches, "svd_ms": svd_ms, "svd_flops": svd_flops,
+                "svd_launches": svd_launches, "clocks": sampler.summary(), "trace": tr, "P": P}
+
+    # ---- timed, device-resident: the measured path, then the plain FP64 path on the same
+    # layers from the same state (the metric's denominator)
+    mine = timed_layers(args.precision, workers)
+    value = replica_rate(n_bs, world, mine["seconds"])
+    plain = None
+    if args.precision != "fp64" and not args.no_plain:
+        plain = timed_layers("fp64", 8)
+        plain["value"] = replica_rate(n_bs, world, plain["seconds"])
+    if world > 1:
+        dist.barrier()
+
+    # ---- end to end through the public API with host buffers, over the same K layers: per
+    # step (layer) the state is copied host -> device and loaded, the layer runs, the state
+    # is stored and copied device -> host (the next step's input) and the trace is read
+    sim.load(g0, l0, c0)
+    sim.set_precision(args.precision)
+    sim.set_workers(workers)
+    run_layers(sim, args.start_layer, args.warmup)
+    g1, l1, c1 = sim.store()
+    host_in = [g1.cpu().pin_memory(), l1.cpu().pin_memory(), c1.cpu().pin_memory()]
+    host_out = [torch.empty_like(x, pin_memory=True) for x in host_in]
+    dev = [torch.empty_like(x) for x in (g1, l1, c1)]
+    del g1, l1, c1
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for i in range(e2e_steps):
-        g_dev.copy_(g_host, non_blocking=True)
-        l_dev.copy_(l_host, non_blocking=True)
-        c_dev.copy_(c_host, non_blocking=True)
-        sim.load(g_dev, l_dev, c_dev)
-        run_layer(args.start_layer + i)
-        g1, l1, c1 = sim.store()
-        g_out.copy_(g1, non_blocking=True)
-        tr = sim.trace()
-    torch.cuda.synchronize()
+    for i in range(args.steps):
+        for dd, hh in zip(dev, host_in):
+            dd.copy_(hh, non_blocking=True)
+        sim.load(*dev)
+        run_layers(sim, first + i, 1, partial=True)
+        gs, ls, cs = sim.store()
+        for hh, dd in zip(host_out, (gs, ls, cs)):
+            hh.copy_(dd, non_blocking=True)
+        tr_e2e = sim.trace()
+        torch.cuda.synchronize()
+        host_in, host_out = host_out, host_in
     t_e2e = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
-    n_bs_e2e = sum(len(layers[args.start_layer + i]) for i in range(e2e_steps))
-    h2d = (g_host.numel() * 16 + l_host.numel() * 8 + c_host.numel() * 4) * e2e_steps
-    d2h = (g_out.numel() * 16 + 16) * e2e_steps
+    state_bytes = sum(x.numel() * x.element_size() for x in host_in)
+    h2d = state_bytes * args.steps
+    d2h = (state_bytes + 16) * args.steps
+    del dev, host_in, host_out
 
-    # ---- the whole circuit: every update from the initial state, the output phases and
-    # the observables (trace, marginals), in one run_mesh call, on a second handle
+    # ---- the whole circuit: every update from the initial state, the output phases and the
+    # observables (trace, marginals), one run_mesh call, on the measured path and on the
+    # plain FP64 path; the probability error is the largest marginal difference / trace
     circuit = None
     if not args.no_circuit and not args.bs_slice:
-        with engine.MPOSimulator(w["n"], w["d"], w["chi"]) as full:
-            full.init_single_photons(range(0, w["n"], 2), w["eta"])
-            torch.cuda.synchronize()
-            if world > 1:
-                dist.barrier()
-            t0 = time.perf_counter()
-            full.run_mesh([b[1] for b in bs], [b[2] for b in bs], [b[3] for b in bs])
-            full.apply_phases(out_phases)
-            trace_c, _ = full.observables()
-            torch.cuda.synchronize()
-            t_circ = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
-        circuit = {"bs_updates": len(bs), "seconds": round(t_circ, 3),
-                   "value": replica_rate(len(bs), world, t_circ), "unit": "BS-updates/s",
-                   "trace": float(trace_c.real),
+        runs = {}
+        for prec in ([args.precision] + (["fp64"] if args.precision != "fp64" and not args.no_plain else [])):
+            with engine.MPOSimulator(w["n"], w["d"], w["chi"]) as full:
+                full.set_precision(prec)
+                full.set_workers(workers if prec == args.precision else 8)
+                full.init_single_photons(range(0, w["n"], 2), w["eta"])
+                torch.cuda.synchronize()
+                if world > 1:
+                    dist.barrier()
+                t0 = time.perf_counter()
+                full.run_mesh([b[1] for b in bs], [b[2] for b in bs], [b[3] for b in bs])
+                tw = full.mesh_truncation()
+                full.apply_phases(out_phases)
+                trace_c, P_c = full.observables()
+                torch.cuda.synchronize()
+                runs[prec] = (max_over_ranks(time.perf_counter() - t0, dist, "cuda"), trace_c, P_c, tw)
+        t_c, trace_c, P_c, tw_c = runs[args.precision]
+        circuit = {"bs_updates": len(bs), "seconds": round(t_c, 3),
+                   "value": replica_rate(len(bs), world, t_c), "unit": "BS-updates/s",
+                   "trace": float(trace_c.real), "max_truncation_weight": float(np.max(tw_c)),
                    "covers": "all updates from the initial state, output phases, trace and marginals "
                              "(host wall clock, initial state excluded)"}
+        if "fp64" in runs and args.precision != "fp64":
+            t_p, trace_p, P_p, tw_p = runs["fp64"]
+            circuit["plain_fp64_seconds"] = round(t_p, 3)
+            circuit["plain_fp64_value"] = replica_rate(len(bs), world, t_p)
+            circuit["prob_err_vs_fp64"] = float(np.abs(P_c - P_p).max() / abs(trace_p))
+            circuit["trace_err_vs_fp64"] = float(abs(trace_c - trace_p) / abs(trace_p))
+            circuit["truncation_weight_err_vs_fp64"] = float(np.abs(tw_c - tw_p).max())
 
-    # ---- roofline of the dominant kernel (the Jacobi round), FP64 against measured DGEMM
+    # ---- roofline of the dominant phase: the SVD step (Jacobi rounds, or the Gram GEMM,
+    # Householder reduction and bisection of the Gram route), FP64 against measured DGEMM
     fp64_peak = measure_fp64_peak(torch) if rank == 0 else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import mpo as _mpo
-        g, l, c = sim.store()
-        # the oracle times the same layers from the same mid-circuit state (input data
-        # only; the timed CPU work is the oracle's own update)
+        g, l, c = g0, l0, c0
+        # the oracle times the layers after the start state (input data only; the timed
+        # CPU work is the oracle's own update)
         st = _mpo.MPOState(w["n"], w["d"], w["chi"], g.cpu().numpy(), l.cpu().numpy(), c.cpu().numpy())
         cpu = cpu_sample(args.cpu_budget, [[(m, th, p) for (m, th, p) in L] for L in layers],
-                         start_layer=args.start_layer + 1, state=st)
+                         start_layer=args.start_layer, state=st)
     if rank == 0:
-        # the updates of a layer overlap on several streams, so the Jacobi phases' flops are
-        # taken over the whole timed region (device time), not over their summed durations
-        achieved = jac_flops / t_dev / 1e12 if t_dev > 0 else None
-        clocks = sampler.summary()
+        # the updates overlap on several streams, so the SVD phases' flops are taken over the
+        # whole timed region (device time), not over their summed per-stream durations
+        achieved = mine["svd_flops"] / mine["seconds"] / 1e12 if mine["seconds"] > 0 else None
+        layer_err = None
+        if plain is not None:
+            layer_err = float(np.abs(mine["P"] - plain["P"]).max() / abs(plain["trace"]))
         line = {
             "metric": METRIC, "value": value, "unit": "BS-updates/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_dev / args.steps * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mine["seconds"] / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": DTYPES[args.precision],
             "data": "synthetic",
-            "config": {"workload": w["name"], "step": "one brick-wall layer (31-32 BS updates); the K timed layers go in one run_mesh call",
-                       "workers": int(os.environ.get("BSMPO_WORKERS", "8")),
-                       "timed_layers": [first, first + args.steps - 1], "bs_updates_timed": n_bs,
-                       "bond_dims_at_start": [min(dims), max(dims)],
-                       "setup_layers_s": round(t_setup, 2),
-                       "circuit_time_s_upper_est": round(len(bs) / (value / world), 1),
-                       "parallelism": "replicas" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (state %.2f GB)" % (g_host.numel() * 16 / 1e9),
-                       "bs_slice": args.bs_slice or "whole layer",
-                       "cutoff": 0.0},
-            "e2e": {"value": replica_rate(n_bs_e2e, world, t_e2e), "unit": "BS-updates/s",
-                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-            "gpu_launches": int(launches),
-            "roofline": {"kernel": "jacobi_gram_kernel + jacobi_apply_kernel (one-sided Jacobi SVD rounds)",
+            "config": config_dict(args, workers),
+            "path": "%s, %d concurrent updates" % (args.precision, workers),
+            "step": "one brick-wall layer (31-32 BS updates) of layers %d-%d; the K timed layers go in one "
+                    "run_mesh call" % (first, first + args.steps - 1),
+            "plain_fp64": None if plain is None else {
+                "value": plain["value"], "unit": "BS-updates/s", "ms_per_step": plain["seconds"] / args.steps * 1e3,
+                "speedup": value / plain["value"], "launches": plain["launches"],
+                "prob_err_after_timed_layers": layer_err,
+                "note": "the same K layers from the same start state on the plain path (one-sided Jacobi SVD, "
+                        "equal to the CPU oracle at 1e-10)"},
+            "e2e": {"value": replica_rate(n_bs, world, t_e2e), "unit": "BS-updates/s",
+                    "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
+                    "covers": "K steps, each: state host->device, load, one layer, store, device->host, trace"},
+            "gpu_launches": int(mine["launches"]),
+            "roofline": {"kernel": SVD_KERNELS[args.precision],
                          "bound": "tensor", "achieved": achieved, "peak": fp64_peak,
                          "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if achieved and fp64_peak else None,
                          "peak_source": "FP64 DGEMM measured in this run (torch.matmul 8192^3, best of 5)",
-                         "achieved_over": "timed region (device time); Jacobi phases of the concurrent updates overlap",
-                         "jacobi_stream_ms_sum": jac_ms, "jacobi_launches": jac_launches,
-                         # DRAM bytes (read + write) of one early-round jacobi_gram_kernel
-                         # launch of this workload, measured with ncu (cold cache)
-                         "traffic": 21995008 if args.workload == "chi1024" else None,
-                         "traffic_unit": "bytes per launch"},
-            "clocks": clocks,
+                         "achieved_over": "timed region (device time); the SVD phases of concurrent updates overlap",
+                         "svd_stream_ms_sum": mine["svd_ms"], "svd_launches": mine["svd_launches"],
+                         "traffic": None},
+            "clocks": mine["clocks"],
             "circuit": circuit,
             "cpu_baseline": cpu,
         }

@@ -667,6 +667,18 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   CK(h, cudaMemcpyAsync(htw, trunc_d, sizeof(double), cudaMemcpyDeviceToHost, st));
   CK(h, host_wait(h));
   const int total_kept = hk[ns];
+  if (gram && h->timing) {
+    // eigen phase of the Gram route (Gram GEMM, tridiagonalisation, bisection): both
+    // events completed before the kept counts arrived
+    float ms = 0.f;
+    CK(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->jac_ms += ms;
+    h->jac_launches += 4;
+    // algorithmic flops: the Gram (8 k^2 rows, complex MACs) and the Householder
+    // reduction of a k x k Hermitian matrix (16/3 k^3, LAPACK's zhetrd count)
+    for (const SectorDesc& S : P.sd)
+      h->jac_flops += 8.0 * (double)S.k * S.k * S.rows_g + 16.0 / 3.0 * (double)S.k * S.k * S.k;
+  }
   if ((rc = clk.mark(4))) return rc;
   // 5. V (Jacobi: extracted from the converged columns; Gram route: eigenvectors, and
   // V = T Y diag(1/sigma) where X = T) and W = V^H C

@@ -181,13 +181,15 @@ int bsmpo_bond_dims(const bsmpo_ctx* h, int* dims);
 /* Number of kernels this handle has launched since creation. */
 int64_t bsmpo_kernel_launches(const bsmpo_ctx* h);
 
-/* Time the Jacobi SVD phase of every update with CUDA events on the handle's stream
- * (on != 0 enables and resets the counters; no extra synchronisation is added). */
+/* Time the SVD phase of every update with CUDA events on the handle's stream: the
+ * Jacobi rounds (BSMPO_PRECISION_FP64) or the Gram + tridiagonalisation + bisection
+ * kernels (Gram route).  on != 0 enables and resets the counters. */
 int bsmpo_set_timing(bsmpo_ctx* h, int on);
 
-/* Accumulated Jacobi-phase device time (ms), its algorithmic flops (executed sweeps:
- * pair Gram + rotation of each 32-column block pair, 8 flops per complex MAC) and
- * the number of Jacobi round launches since bsmpo_set_timing(h, 1). */
+/* Accumulated SVD-phase device time (ms), its algorithmic flops and its launches since
+ * bsmpo_set_timing(h, 1).  Jacobi: executed sweeps, pair Gram + rotation of each
+ * 32-column block pair; Gram route: 8 k^2 rows (the Gram) + 16/3 k^3 (Householder
+ * reduction) per sector; 8 flops per complex MAC. */
 int bsmpo_jacobi_timing(const bsmpo_ctx* h, double* ms, double* flops, int64_t* launches);
 
 /* Stage timing, filled only when the handle was created with BSMPO_PROFILE=1 in the
