@@ -374,6 +374,7 @@ def main():
         torch.cuda.synchronize()
         sim.set_timing(True)
         launches0 = sim.kernel_launches()
+        routes0 = sim.svd_routes()
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
@@ -388,12 +389,14 @@ def main():
         torch.cuda.nvtx.range_pop()
         sampler.stop()
         launches = sim.kernel_launches() - launches0
+        routes = [a - b for a, b in zip(sim.svd_routes(), routes0)]
         svd_ms, svd_flops, svd_launches = sim.jacobi_timing()
         sim.set_timing(False)
         t = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, "cuda")
         tr, P = sim.observables()
         return {"seconds": t, "launches": launches, "svd_ms": svd_ms, "svd_flops": svd_flops,
-                "svd_launches": svd_launches, "clocks": sampler.summary(), "trace": tr, "P": P}
+                "svd_launches": svd_launches, "clocks": sampler.summary(), "trace": tr, "P": P,
+                "routes": {"jacobi": routes[0], "gram": routes[1]}}
 
     # ---- timed, device-resident: the measured path, then the plain FP64 path on the same
     # layers from the same state (the metric's denominator)
@@ -512,6 +515,7 @@ def main():
                     "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
                     "covers": "K steps, each: state host->device, load, one layer, store, device->host, trace"},
             "gpu_launches": int(mine["launches"]),
+            "svd_routes": mine["routes"],
             "roofline": {"kernel": SVD_KERNELS[args.precision],
                          "bound": "tensor", "achieved": achieved, "peak": fp64_peak,
                          "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if achieved and fp64_peak else None,

@@ -43,6 +43,7 @@ SIGNATURES = {
     "bsmpo_last_update_work": (_c_int, [_vp, _dp, _dp, _dp]),
     "bsmpo_bond_dims": (_c_int, [_vp, _ip]),
     "bsmpo_kernel_launches": (ctypes.c_int64, [_vp]),
+    "bsmpo_svd_routes": (_c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "bsmpo_stage_times": (_c_int, [_vp, _dp, _c_int]),
     "bsmpo_set_timing": (_c_int, [_vp, _c_int]),
     "bsmpo_jacobi_timing": (_c_int, [_vp, _dp, _dp, ctypes.POINTER(ctypes.c_int64)]),

@@ -105,6 +105,7 @@ struct bsmpo_ctx {
   const bsmpo_ctx* diag = nullptr;
   int last_index = -1;    // worker: mesh index of the last update it ran
   std::vector<double> mesh_tw;   // truncation weight of every update of the last mesh
+  int64_t route_count[2] = {0, 0};   // updates solved by Jacobi [0] and by the Gram route [1]
 };
 
 namespace {
@@ -498,7 +499,21 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   const MixPair* pairs_d = reinterpret_cast<const MixPair*>(dt + L.pairs);
   const GemmGroup* gg_d = reinterpret_cast<const GemmGroup*>(dt + L.gg);
   const GemmGroup* ggram_d = reinterpret_cast<const GemmGroup*>(dt + L.ggram);
-  const bool gram = h->precision != BSMPO_PRECISION_FP64;
+  // The Gram route drops singular values below ~2e-6 of a sector's largest.  Where the
+  // update does not truncate to chi that is pure loss (W = V^H C carries them through
+  // 1 / Lambda_R), so such updates take the exact Jacobi SVD: up front when the
+  // candidates cannot exceed chi or the centre bond holds fewer than chi vectors, and
+  // after the selection when fewer than chi survive.
+  bool gram = h->precision != BSMPO_PRECISION_FP64;
+  {
+    // the centre bond's current dimension predicts the outcome: a bond below chi was not
+    // truncated by the last update on it and is unlikely to be by this one
+    int64_t sum_k = 0, centre = 0;
+    for (const SectorDesc& S : P.sd) sum_k += S.k;
+    const std::vector<int>& cm = mirror(h);
+    for (int q = 0; q < dd; ++q) centre += cm[(size_t)(mode + 1) * dd + q];
+    if (sum_k <= chi || centre < chi) gram = false;
+  }
   const JacobiWork* jw_d = reinterpret_cast<const JacobiWork*>(dt + L.jw);
   const int64_t chi2 = (int64_t)chi * chi;
 
@@ -517,6 +532,10 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   double* lam_d = nullptr;
   double* dbuf_d = nullptr;
   double* ebuf_d = nullptr;
+  int* hk = reinterpret_cast<int*>(h->hres.p);
+  double* htw = reinterpret_cast<double*>(static_cast<char*>(h->hres.p) + 512);
+  int total_kept = 0;
+  for (;;) {
   if (gram) {
     if (P.max_k > eigen_max_k())
       return fail(h, BSMPO_ECAPACITY, "a sector of dimension " + std::to_string(P.max_k) +
@@ -661,12 +680,20 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
                                               align_up((size_t)(ns + 1) * sizeof(int), 16));
   CKL(h, launch_select(tab_d, sd_d, ns, reinterpret_cast<double*>(h->sig.p),
                        reinterpret_cast<double*>(h->keys.p), h->cutoff, chi, kept_d, trunc_d, st));
-  int* hk = reinterpret_cast<int*>(h->hres.p);
-  double* htw = reinterpret_cast<double*>(static_cast<char*>(h->hres.p) + 512);
   CK(h, cudaMemcpyAsync(hk, kept_d, (size_t)(ns + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(h, cudaMemcpyAsync(htw, trunc_d, sizeof(double), cudaMemcpyDeviceToHost, st));
   CK(h, host_wait(h));
-  const int total_kept = hk[ns];
+  total_kept = hk[ns];
+  if (gram && total_kept < chi && h->cutoff == 0.0) {
+    // not truncated to chi: redo the SVD exactly (the Gram matrix and the eigen buffers
+    // are not needed any more; the Jacobi matrix is intact)
+    gram = false;
+    CKL(h, launch_identity_rows(sd_d, ns, P.max_left_m2, h->abuf.p, st));
+    continue;
+  }
+  break;
+  }
+  h->route_count[gram ? 1 : 0]++;
   if (gram && h->timing) {
     // eigen phase of the Gram route (Gram GEMM, tridiagonalisation, bisection): both
     // events completed before the kept counts arrived
@@ -961,6 +988,7 @@ int run_mesh_concurrent(bsmpo_ctx* h, int n_bs, const int* modes, const cplx* u3
     h->launches += w->launches;
     h->updates += w->updates;
     h->jacobi_rounds += w->jacobi_rounds;
+    for (int q = 0; q < 2; ++q) { h->route_count[q] += w->route_count[q]; w->route_count[q] = 0; }
     h->jac_ms += w->jac_ms;
     h->jac_flops += w->jac_flops;
     h->jac_launches += w->jac_launches;
@@ -1409,6 +1437,13 @@ int bsmpo_bond_dims(const bsmpo_ctx* h, int* dims) {
 }
 
 int64_t bsmpo_kernel_launches(const bsmpo_ctx* h) { return h ? h->launches : 0; }
+
+int bsmpo_svd_routes(const bsmpo_ctx* h, int64_t* counts) {
+  if (!h || !counts) return fail(nullptr, BSMPO_EINVAL, "bad argument");
+  counts[0] = h->route_count[0];
+  counts[1] = h->route_count[1];
+  return BSMPO_OK;
+}
 
 int bsmpo_set_timing(bsmpo_ctx* h, int on) {
   if (!h) return fail(nullptr, BSMPO_EINVAL, "null handle");

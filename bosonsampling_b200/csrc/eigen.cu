@@ -72,9 +72,9 @@ __device__ __forceinline__ cplx cdiv(cplx a, cplx b) {
 //        w'_i conj(v'_l) (v', w' of step j - 1), write back, p_i = tau sum_l A[i][l] v_l;
 //        partial c = sum conj(p_i) v_i;
 //    --  cluster barrier
-//    S2  c = sum of the partials; w_i = p_i - tau c / 2 v_i on its rows; publish;
-//    --  cluster barrier
-//    S3  gather the whole w_j (it is v', w' of the next step).
+//    S2  c = sum of the partials; every CTA forms the whole w_j = p - tau c / 2 v from
+//        the owners' p (it is v', w' of the next step).
+//    Two cluster barriers per step; S0 is one warp's work.
 // Every row is read and written by its owner only, so the trailing matrix needs no
 // ordering across CTAs; the vectors travel through distributed shared memory.
 __global__ void __cluster_dims__(TD_CL, 1, 1) __launch_bounds__(TD_NT)
@@ -108,27 +108,24 @@ __global__ void __cluster_dims__(TD_CL, 1, 1) __launch_bounds__(TD_NT)
     cplx* vcur = vb + (j & 1) * kmax;
     const cplx* vprev = vb + ((j + 1) & 1) * kmax;
     const cplx* wprev = wb + ((j + 1) & 1) * kmax;
-    // ---- S0: the reflector of row j
-    if (rank == owner) {
+    // ---- S0: the reflector of row j (one warp of the owner; warp shuffles only)
+    if (rank == owner && warp == 0) {
       cplx* row = A + (int64_t)j * k;
       double part = 0.0;
       const cplx vj = j > 0 ? vprev[j] : cmake(0.0, 0.0), wj = j > 0 ? wprev[j] : cmake(0.0, 0.0);
-      for (int l = j + tid; l < k; l += TD_NT) {
+      for (int l = j + lane; l < k; l += 32) {
         cplx a = ldc(row + l);
         if (j > 0) a = csub(a, cadd(cmulc(vj, wprev[l]), cmulc(wj, vprev[l])));
         if (l == j) {
-          if (tid == 0) dd[j] = a.x;
+          dd[j] = a.x;
         } else {
           const cplx x = cconj(a);
           vpub[l - j - 1] = x;          // x for now, scaled below
           if (l > j + 1) part += cabs2(x);
         }
       }
-      part = warp_sum(part);
-      if (lane == 0) scal[8 + warp] = part;
-      __syncthreads();
-      double xn2 = 0.0;
-      for (int w = 0; w < TD_NT / 32; ++w) xn2 += scal[8 + w];   // fixed order: every thread alike
+      const double xn2 = warp_sum(part);   // the same value in every lane
+      __syncwarp();
       const cplx alpha = vpub[0];
       cplx tau, sc;
       double beta;
@@ -141,13 +138,13 @@ __global__ void __cluster_dims__(TD_CL, 1, 1) __launch_bounds__(TD_NT)
         tau = cmake((beta - alpha.x) / beta, -alpha.y / beta);
         sc = cdiv(cmake(1.0, 0.0), cmake(alpha.x - beta, alpha.y));
       }
-      __syncthreads();                  // alpha read by all before vpub[0] changes
-      for (int l = tid; l < t; l += TD_NT) {
+      __syncwarp();                     // alpha read by every lane before vpub[0] changes
+      for (int l = lane; l < t; l += 32) {
         const cplx v = l == 0 ? cmake(1.0, 0.0) : cmul(sc, vpub[l]);
         vpub[l] = v;
         stc(row + j + 1 + l, v);        // v_j kept in row j for the back-transformation
       }
-      if (tid == 0) {
+      if (lane == 0) {
         ee[j] = beta;
         tt[j] = tau;
         scal[2] = tau.x;
@@ -199,7 +196,9 @@ __global__ void __cluster_dims__(TD_CL, 1, 1) __launch_bounds__(TD_NT)
       }
     }
     cluster.sync();
-    // ---- S2: w on the own rows
+    // ---- S2: c from the partials, then the whole w_j = p - tau c / 2 v, each CTA
+    // reading the p of every row from its owner (no further barrier: the next writes of
+    // pown and of the partials follow the next step's first barrier)
     {
       const double* rs = cluster.map_shared_rank(scal, owner);
       const cplx tau = cmake(rs[2], rs[3]);
@@ -210,17 +209,10 @@ __global__ void __cluster_dims__(TD_CL, 1, 1) __launch_bounds__(TD_NT)
         cy += qs[1];
       }
       const cplx a2 = cscale(cmul(tau, cmake(cx, cy)), -0.5);
-      const int i0 = j + 1 + ((rank - (j + 1)) % TD_CL + TD_CL) % TD_CL;
-      for (int i = i0 + tid * TD_CL; i < k; i += TD_CL * TD_NT)
-        wown[i / TD_CL] = cadd(pown[i / TD_CL], cmul(a2, vcur[i]));
-    }
-    cluster.sync();
-    // ---- S3: the whole w_j
-    {
       cplx* wcur = wb + (j & 1) * kmax;
       for (int l = j + 1 + tid; l < k; l += TD_NT) {
-        const cplx* rw = cluster.map_shared_rank(wown, l % TD_CL);
-        wcur[l] = rw[l / TD_CL];
+        const cplx* rp = cluster.map_shared_rank(pown, l % TD_CL);
+        wcur[l] = cadd(rp[l / TD_CL], cmul(a2, vcur[l]));
       }
       __syncthreads();
     }

@@ -232,6 +232,12 @@ class MPOSimulator:
         self._chk(self.L.bsmpo_bond_dims(self.h, _capi.iptr(out)))
         return [int(x) for x in out]
 
+    def svd_routes(self):
+        """(updates solved by the Jacobi SVD, by the Gram route) since creation."""
+        c = (ctypes.c_int64 * 2)()
+        self._chk(self.L.bsmpo_svd_routes(self.h, c))
+        return int(c[0]), int(c[1])
+
     def kernel_launches(self):
         return int(self.L.bsmpo_kernel_launches(self.h))
 

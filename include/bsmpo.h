@@ -90,7 +90,12 @@ int bsmpo_set_stream(bsmpo_ctx* h, void* stream);
  *   BSMPO_PRECISION_FP64_GRAM  FP64 contractions, per-sector Gram matrix and Hermitian
  *                              eigenproblem in FP64 (Householder tridiagonalisation,
  *                              bisection, inverse iteration): singular values below
- *                              about 2e-6 of the largest are dropped as zero. */
+ *                              about 2e-6 of the largest are dropped as zero.  An
+ *                              update whose candidates do not exceed chi, whose centre
+ *                              bond holds fewer than chi vectors, or that keeps fewer
+ *                              than chi after the selection, is solved by the
+ *                              exact Jacobi SVD instead (nothing is truncated there, so
+ *                              the dropped values would be pure loss). */
 #define BSMPO_PRECISION_FP64 0
 #define BSMPO_PRECISION_FP64_GRAM 1
 int bsmpo_set_precision(bsmpo_ctx* h, int precision);
@@ -177,6 +182,10 @@ int bsmpo_last_update_work(const bsmpo_ctx* h, double* gemm_flops, double* svd_f
 
 /* Bond dimensions (occupied slots) of every bond, host int[n+1]. */
 int bsmpo_bond_dims(const bsmpo_ctx* h, int* dims);
+
+/* Updates solved by the Jacobi SVD (counts[0]) and by the Gram route (counts[1]) since
+ * creation (host int64[2]). */
+int bsmpo_svd_routes(const bsmpo_ctx* h, int64_t* counts);
 
 /* Number of kernels this handle has launched since creation. */
 int64_t bsmpo_kernel_launches(const bsmpo_ctx* h);
