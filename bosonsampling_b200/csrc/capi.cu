@@ -75,6 +75,7 @@ struct bsmpo_ctx {
   // Gram / eigen route of the sector SVD (precision != BSMPO_PRECISION_FP64)
   DevBuf gbuf, eigd, taub, invsig, escr, swp, zbuf, ybuf;
   int precision = BSMPO_PRECISION_FP64;
+  int gram_policy = 2;   // BSMPO_GRAM_POLICY: 0 Gram everywhere, 1 + fallback, 2 + prediction
   HostStage stage, stage2, hres;
   // last update diagnostics (host)
   std::vector<int> last_cc, last_shape, last_kept, last_k;
@@ -512,7 +513,7 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
     for (const SectorDesc& S : P.sd) sum_k += S.k;
     const std::vector<int>& cm = mirror(h);
     for (int q = 0; q < dd; ++q) centre += cm[(size_t)(mode + 1) * dd + q];
-    if (sum_k <= chi || centre < chi) gram = false;
+    if (sum_k <= chi || (h->gram_policy >= 2 && centre < chi)) gram = false;
   }
   const JacobiWork* jw_d = reinterpret_cast<const JacobiWork*>(dt + L.jw);
   const int64_t chi2 = (int64_t)chi * chi;
@@ -684,7 +685,7 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   CK(h, cudaMemcpyAsync(htw, trunc_d, sizeof(double), cudaMemcpyDeviceToHost, st));
   CK(h, host_wait(h));
   total_kept = hk[ns];
-  if (gram && total_kept < chi && h->cutoff == 0.0) {
+  if (gram && total_kept < chi && h->cutoff == 0.0 && h->gram_policy >= 1) {
     // not truncated to chi: redo the SVD exactly (the Gram matrix and the eigen buffers
     // are not needed any more; the Jacobi matrix is intact)
     gram = false;
@@ -897,6 +898,7 @@ int run_mesh_concurrent(bsmpo_ctx* h, int n_bs, const int* modes, const cplx* u3
     bsmpo_ctx* w = h->workers[k];
     w->cutoff = h->cutoff;
     w->precision = h->precision;
+    w->gram_policy = h->gram_policy;
     w->jac_rows = h->jac_rows;
     w->timing = h->timing;
     if (w->timing && !w->ev0) {
@@ -1116,6 +1118,8 @@ int bsmpo_create(int n, int d, int chi, int flags, bsmpo_ctx** out) {
   h->profile = prof && prof[0] == '1';
   const char* jr = std::getenv("BSMPO_JACOBI_ROWS");
   if (jr && std::atoi(jr) >= 16) h->jac_rows = std::atoi(jr);
+  const char* gp = std::getenv("BSMPO_GRAM_POLICY");
+  if (gp && gp[0] >= '0' && gp[0] <= '2') h->gram_policy = gp[0] - '0';
   const char* nwk = std::getenv("BSMPO_WORKERS");
   if (nwk && std::atoi(nwk) >= 1 && std::atoi(nwk) <= 64) h->n_workers = std::atoi(nwk);
   *out = h;
