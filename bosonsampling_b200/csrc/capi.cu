@@ -75,7 +75,10 @@ struct bsmpo_ctx {
   // Gram / eigen route of the sector SVD (precision != BSMPO_PRECISION_FP64)
   DevBuf gbuf, eigd, taub, invsig, escr, swp, zbuf, ybuf;
   int precision = BSMPO_PRECISION_FP64;
-  int gram_policy = 2;   // BSMPO_GRAM_POLICY: 0 Gram everywhere, 1 + fallback, 2 + prediction
+  // BSMPO_GRAM_POLICY (Gram route): 0 (default) exact Jacobi only where the candidates
+  // cannot exceed chi; 1 also after a selection that keeps fewer than chi; 2 also where
+  // the centre bond holds fewer than chi vectors
+  int gram_policy = 0;
   HostStage stage, stage2, hres;
   // last update diagnostics (host)
   std::vector<int> last_cc, last_shape, last_kept, last_k;
@@ -187,6 +190,8 @@ struct Plan {
   std::vector<MixPair> pairs;
   std::vector<GemmGroup> gg;
   std::vector<GemmGroup> ggram;   // Gram G_s = X^H X of every sector (Gram route)
+  std::vector<int> tdlist;        // sectors by tridiagonalisation size class (Gram route)
+  int td_count[4] = {0, 0, 0, 0}, td_kmax[4] = {0, 0, 0, 0};
   std::vector<JacobiWork> jw;
   int mix_tiles = 0, gemm_tiles = 0, max_rounds = 0, max_k = 0, max_left_m2 = 0;
   int gram_ctas = 0, apply_ctas = 0, jac_slots = 0;   // every sector in one round
@@ -343,6 +348,17 @@ int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
     P.ggram.push_back(g);
   }
   P.gram_tiles = gtiles;
+  P.tdlist.clear();
+  for (int c = 0; c < 4; ++c) {
+    P.td_count[c] = 0;
+    P.td_kmax[c] = 0;
+    for (int s = 0; s < (int)P.sd.size(); ++s)
+      if (tridiag_class(P.sd[s].k) == c) {
+        P.tdlist.push_back(s);
+        P.td_count[c]++;
+        P.td_kmax[c] = std::max(P.td_kmax[c], P.sd[s].k);
+      }
+  }
   T.n_theta = (int)P.td.size();
   // mix pairs (a >= b)
   P.pairs.clear();
@@ -401,7 +417,7 @@ int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
 
 // packs plan tables into the pinned stage and copies them to the device table buffer
 struct TabLayout {
-  size_t tab, tidx, td, sd, pairs, gg, ggram, jw, total;
+  size_t tab, tidx, td, sd, pairs, gg, ggram, tdlist, jw, total;
 };
 
 TabLayout layout_of(const Plan& P) {
@@ -414,6 +430,7 @@ TabLayout layout_of(const Plan& P) {
   L.pairs = o; o = align_up(o + P.pairs.size() * sizeof(MixPair) + 1, 256);
   L.gg = o; o = align_up(o + P.gg.size() * sizeof(GemmGroup) + 1, 256);
   L.ggram = o; o = align_up(o + P.ggram.size() * sizeof(GemmGroup) + 1, 256);
+  L.tdlist = o; o = align_up(o + P.tdlist.size() * sizeof(int) + 1, 256);
   L.jw = o; o = align_up(o + P.jw.size() * sizeof(JacobiWork) + 1, 256);
   L.total = o;
   return L;
@@ -487,6 +504,7 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   put(hs, L.pairs, P.pairs);
   put(hs, L.gg, P.gg);
   put(hs, L.ggram, P.ggram);
+  put(hs, L.tdlist, P.tdlist);
   std::vector<JacobiWork> active(P.jw);
   int gram_ctas = 0, apply_ctas = 0, slots = 0;
   jacobi_launch_list(active, &gram_ctas, &apply_ctas, &slots);
@@ -500,6 +518,7 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   const MixPair* pairs_d = reinterpret_cast<const MixPair*>(dt + L.pairs);
   const GemmGroup* gg_d = reinterpret_cast<const GemmGroup*>(dt + L.gg);
   const GemmGroup* ggram_d = reinterpret_cast<const GemmGroup*>(dt + L.ggram);
+  const int* tdlist_d = reinterpret_cast<const int*>(dt + L.tdlist);
   // The Gram route drops singular values below ~2e-6 of a sector's largest.  Where the
   // update does not truncate to chi that is pure loss (W = V^H C carries them through
   // 1 / Lambda_R), so such updates take the exact Jacobi SVD: up front when the
@@ -551,7 +570,8 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
     if (h->timing) CK(h, cudaEventRecord(h->ev0, st));
     CKL(h, launch_zgemm_grouped(h->abuf.p, h->abuf.p, h->gbuf.p, nullptr, ggram_d, (int)P.ggram.size(),
                                 P.gram_tiles, st));
-    CKL(h, launch_tridiag(sd_d, ns, P.max_k, h->gbuf.p, dbuf_d, ebuf_d, h->taub.p, st));
+    CK(h, launch_tridiag(sd_d, tdlist_d, P.td_count, P.td_kmax, h->gbuf.p, dbuf_d, ebuf_d, h->taub.p, st));
+    for (int c = 0; c < 4; ++c) h->launches += P.td_count[c] > 0;
     CK(h, launch_bisect(sd_d, ns, P.max_k, dbuf_d, ebuf_d, lam_d, reinterpret_cast<double*>(h->sig.p),
                         reinterpret_cast<double*>(h->invsig.p), st));
     h->launches += 2;

@@ -31,12 +31,12 @@ namespace cg = cooperative_groups;
 namespace {
 
 constexpr double EPS = 2.220446049250313e-16;
-constexpr int TD_CL = 8;     // CTAs per sector (one cluster)
 constexpr int TD_NT = 256;
+constexpr int TD_CLASSES = 4;   // cluster sizes 1, 2, 4, 8 CTAs per sector, by sector size
 
 // dynamic shared memory of the tridiagonalisation (kmax = largest k of the launch)
-__host__ __device__ inline size_t td_smem_bytes(int kmax) {
-  const int own = kmax / TD_CL + 1;
+__host__ __device__ inline size_t td_smem_bytes(int kmax, int cl) {
+  const int own = kmax / cl + 1;
   return sizeof(cplx) * ((size_t)5 * kmax + 2 * (size_t)own) + 64 * sizeof(double);
 }
 
@@ -62,8 +62,9 @@ __device__ __forceinline__ cplx cdiv(cplx a, cplx b) {
 }
 
 // ---------------------------------------------------------------------------------
-// 1. Tridiagonalisation.  Cluster c handles sector c; CTA `rank` owns the rows
-//    i = rank (mod TD_CL).  Per step j (trailing size t = k - j - 1):
+// 1. Tridiagonalisation.  Cluster c handles sector list[c]; its cl CTAs (1, 2, 4 or 8,
+//    by sector size: a small sector would spend its steps waiting at barriers of a big
+//    cluster) own the rows i = rank (mod cl).  Per step j (trailing size t = k - j - 1):
 //    S0  owner of row j: apply the pending update of step j - 1 to row j, form the
 //        reflector from x = conj(A[j][j+1:]) (zlarfg: beta real), store v_j in row j,
 //        d_j, e_j = beta, tau_j; publish v_j and tau_j in its shared memory;
@@ -77,12 +78,14 @@ __device__ __forceinline__ cplx cdiv(cplx a, cplx b) {
 //    Two cluster barriers per step; S0 is one warp's work.
 // Every row is read and written by its owner only, so the trailing matrix needs no
 // ordering across CTAs; the vectors travel through distributed shared memory.
-__global__ void __cluster_dims__(TD_CL, 1, 1) __launch_bounds__(TD_NT)
-    tridiag_kernel(const SectorDesc* __restrict__ sd, int kmax, cplx* __restrict__ gbuf,
-                   double* __restrict__ dbuf, double* __restrict__ ebuf, cplx* __restrict__ taubuf) {
+__global__ void __launch_bounds__(TD_NT)
+    tridiag_kernel(const SectorDesc* __restrict__ sd, const int* __restrict__ list, int kmax,
+                   cplx* __restrict__ gbuf, double* __restrict__ dbuf, double* __restrict__ ebuf,
+                   cplx* __restrict__ taubuf) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
+  const int TD_CL = (int)cluster.num_blocks();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int own_cap = kmax / TD_CL + 1;
   // v and w of two consecutive steps (ping-pong): vb + (j & 1) kmax, wb + (j & 1) kmax
@@ -90,9 +93,8 @@ __global__ void __cluster_dims__(TD_CL, 1, 1) __launch_bounds__(TD_NT)
   cplx* wb = vb + 2 * kmax;
   cplx* vpub = wb + 2 * kmax;          // v_j as published by the owner (index l: column j+1+l)
   cplx* pown = vpub + kmax;            // p_i of the own rows (local index i / TD_CL)
-  cplx* wown = pown + own_cap;         // w_i of the own rows
-  double* scal = reinterpret_cast<double*>(wown + own_cap);   // [0..1] cpart, [2..3] tau, [8..] reduction
-  const SectorDesc& S = sd[blockIdx.x / TD_CL];
+  double* scal = reinterpret_cast<double*>(pown + 2 * own_cap);   // [0..1] cpart, [2..3] tau, [8..] reduction
+  const SectorDesc& S = sd[list[blockIdx.x / TD_CL]];
   const int k = S.k;                   // the same for every CTA of the cluster
   cplx* A = gbuf + S.g_off;
   double* dd = dbuf + S.s_off;
@@ -523,23 +525,46 @@ __global__ __launch_bounds__(BT_NT) void backtransform_kernel(const SectorDesc* 
 }  // namespace
 
 int eigen_max_k() {
-  // shared memory of the tridiagonalisation: (5 k + 2 (k / 8 + 1)) x 16 B <= 227 KB
+  // shared memory of the tridiagonalisation: (5 k + 2 (k + 1)) x 16 B <= 227 KB with one
+  // CTA per sector
   int k = 256;
-  while (td_smem_bytes(k + 256) <= 227 * 1024) k += 256;
+  while (td_smem_bytes(k + 256, 1) <= 227 * 1024) k += 256;
   return std::min(k, 32 * 32);   // the back-transformation keeps 32 entries per lane
 }
 
-cudaError_t launch_tridiag(const SectorDesc* sd_dev, int n_sectors, int kmax, void* gbuf,
-                           double* dbuf, double* ebuf, void* taubuf, cudaStream_t s) {
-  if (n_sectors <= 0) return cudaSuccess;
-  const size_t smem = td_smem_bytes(kmax);
+int tridiag_class(int k) { return k <= 64 ? 0 : k <= 160 ? 1 : k <= 320 ? 2 : 3; }
+
+cudaError_t launch_tridiag(const SectorDesc* sd_dev, const int* list_dev, const int* class_count,
+                           const int* class_kmax, void* gbuf, double* dbuf, double* ebuf,
+                           void* taubuf, cudaStream_t s) {
   // once per process: the largest dynamic shared memory any launch may ask for
   static const cudaError_t attr = cudaFuncSetAttribute(
-      tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)td_smem_bytes(eigen_max_k()));
+      tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)td_smem_bytes(eigen_max_k(), 1));
   if (attr != cudaSuccess) return attr;
-  tridiag_kernel<<<n_sectors * TD_CL, TD_NT, smem, s>>>(sd_dev, kmax, reinterpret_cast<cplx*>(gbuf),
-                                                        dbuf, ebuf, reinterpret_cast<cplx*>(taubuf));
-  return cudaGetLastError();
+  int first = 0;
+  for (int c = 0; c < TD_CLASSES; ++c) {
+    const int count = class_count[c];
+    if (count == 0) continue;
+    const int cl = 1 << c;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(count * cl);
+    cfg.blockDim = dim3(TD_NT);
+    cfg.dynamicSmemBytes = td_smem_bytes(class_kmax[c], cl);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, tridiag_kernel, sd_dev, list_dev + first, class_kmax[c],
+                                       reinterpret_cast<cplx*>(gbuf), dbuf, ebuf,
+                                       reinterpret_cast<cplx*>(taubuf));
+    if (e != cudaSuccess) return e;
+    first += count;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_bisect(const SectorDesc* sd_dev, int n_sectors, int kmax, const double* dbuf,

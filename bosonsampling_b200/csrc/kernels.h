@@ -162,8 +162,13 @@ cudaError_t launch_jacobi_finish(const SectorDesc* sd_dev, int n_sectors, int ma
 // Gram / Hermitian-eigen route of the sector SVD (see eigen.cu).  gbuf holds every
 // sector's Gram G = X^H X (k x k at g_off), overwritten by the Householder vectors.
 int eigen_max_k();
-cudaError_t launch_tridiag(const SectorDesc* sd_dev, int n_sectors, int kmax, void* gbuf,
-                           double* dbuf, double* ebuf, void* taubuf, cudaStream_t s);
+// Sectors go in four launches by size class (tridiag_class: 1, 2, 4 or 8 CTAs per
+// sector): list_dev holds the sector indices grouped by class, class_count / class_kmax
+// (host, 4 entries) the number of sectors and their largest k per class.
+int tridiag_class(int k);
+cudaError_t launch_tridiag(const SectorDesc* sd_dev, const int* list_dev, const int* class_count,
+                           const int* class_kmax, void* gbuf, double* dbuf, double* ebuf,
+                           void* taubuf, cudaStream_t s);
 // eigenvalues (lam, descending), singular values sig = sqrt(lam) (0 below the floor), 1/sig
 cudaError_t launch_bisect(const SectorDesc* sd_dev, int n_sectors, int kmax, const double* dbuf,
                           const double* ebuf, double* lam, double* sig, double* invsig,

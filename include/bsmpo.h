@@ -91,11 +91,15 @@ int bsmpo_set_stream(bsmpo_ctx* h, void* stream);
  *                              eigenproblem in FP64 (Householder tridiagonalisation,
  *                              bisection, inverse iteration): singular values below
  *                              about 2e-6 of the largest are dropped as zero.  An
- *                              update whose candidates do not exceed chi, whose centre
- *                              bond holds fewer than chi vectors, or that keeps fewer
- *                              than chi after the selection, is solved by the
- *                              exact Jacobi SVD instead (nothing is truncated there, so
- *                              the dropped values would be pure loss). */
+ *                              update whose candidates cannot exceed chi (the growing
+ *                              bonds of the first layers) is solved by the exact Jacobi
+ *                              SVD instead: nothing is truncated there, and dropping
+ *                              small values there is pure loss (W = V^H C carries them
+ *                              through 1 / Lambda_R).  The environment variable
+ *                              BSMPO_GRAM_POLICY, read at create, widens that rule:
+ *                              1 adds updates that keep fewer than chi after the
+ *                              selection (the SVD is redone), 2 also those whose centre
+ *                              bond holds fewer than chi vectors. */
 #define BSMPO_PRECISION_FP64 0
 #define BSMPO_PRECISION_FP64_GRAM 1
 int bsmpo_set_precision(bsmpo_ctx* h, int precision);
