@@ -75,6 +75,10 @@ struct bsmpo_ctx {
   // Gram / eigen route of the sector SVD (precision != BSMPO_PRECISION_FP64)
   DevBuf gbuf, eigd, taub, invsig, escr, swp, zbuf, ybuf;
   int precision = BSMPO_PRECISION_FP64;
+  // the tridiagonalisation's size classes run side by side: three more streams, forked
+  // from and joined to `stream` with events
+  cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t fork_ev = nullptr, join_ev[3] = {nullptr, nullptr, nullptr};
   // BSMPO_GRAM_POLICY (Gram route): 0 (default) exact Jacobi only where the candidates
   // cannot exceed chi; 1 also after a selection that keeps fewer than chi; 2 also where
   // the centre bond holds fewer than chi vectors
@@ -570,8 +574,26 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
     if (h->timing) CK(h, cudaEventRecord(h->ev0, st));
     CKL(h, launch_zgemm_grouped(h->abuf.p, h->abuf.p, h->gbuf.p, nullptr, ggram_d, (int)P.ggram.size(),
                                 P.gram_tiles, st));
-    CK(h, launch_tridiag(sd_d, tdlist_d, P.td_count, P.td_kmax, h->gbuf.p, dbuf_d, ebuf_d, h->taub.p, st));
-    for (int c = 0; c < 4; ++c) h->launches += P.td_count[c] > 0;
+    {
+      if (!h->fork_ev) {
+        CK(h, cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
+        for (int i = 0; i < 3; ++i) {
+          CK(h, cudaStreamCreateWithFlags(&h->aux[i], cudaStreamNonBlocking));
+          CK(h, cudaEventCreateWithFlags(&h->join_ev[i], cudaEventDisableTiming));
+        }
+      }
+      const cudaStream_t ts[4] = {st, h->aux[0], h->aux[1], h->aux[2]};
+      CK(h, cudaEventRecord(h->fork_ev, st));
+      for (int i = 0; i < 3; ++i)
+        if (P.td_count[2 - i] > 0) CK(h, cudaStreamWaitEvent(h->aux[i], h->fork_ev, 0));
+      CK(h, launch_tridiag(sd_d, tdlist_d, P.td_count, P.td_kmax, h->gbuf.p, dbuf_d, ebuf_d, h->taub.p, ts));
+      for (int i = 0; i < 3; ++i)
+        if (P.td_count[2 - i] > 0) {
+          CK(h, cudaEventRecord(h->join_ev[i], h->aux[i]));
+          CK(h, cudaStreamWaitEvent(st, h->join_ev[i], 0));
+        }
+      for (int c = 0; c < 4; ++c) h->launches += P.td_count[c] > 0;
+    }
     CK(h, launch_bisect(sd_d, ns, P.max_k, dbuf_d, ebuf_d, lam_d, reinterpret_cast<double*>(h->sig.p),
                         reinterpret_cast<double*>(h->invsig.p), st));
     h->launches += 2;
@@ -871,6 +893,11 @@ void free_workspaces(bsmpo_ctx* h) {
   if (h->wait_ev) cudaEventDestroy(h->wait_ev);
   for (cudaEvent_t& e : h->poll_ev)
     if (e) cudaEventDestroy(e);
+  if (h->fork_ev) cudaEventDestroy(h->fork_ev);
+  for (int i = 0; i < 3; ++i) {
+    if (h->aux[i]) { cudaStreamSynchronize(h->aux[i]); cudaStreamDestroy(h->aux[i]); }
+    if (h->join_ev[i]) cudaEventDestroy(h->join_ev[i]);
+  }
 }
 
 // A worker context for concurrent updates: the owner's state, its own stream.

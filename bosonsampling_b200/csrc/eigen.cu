@@ -298,6 +298,7 @@ __global__ __launch_bounds__(BI_NT) void bisect_kernel(const SectorDesc* __restr
   const int target = k - 1 - i;        // eigenvalues below lambda_(i) (ascending index)
   const double pivmin = bounds[2];
   double a = bounds[0], b = bounds[1];
+  const double tol_abs = 4.0 * EPS * fmax(fabs(a), fabs(b)) + 2.0 * pivmin;
   for (int it = 0; it < 16; ++it) {
     const double x = a + (double)(lane + 1) * ((b - a) / 33.0);
     const int c = sturm_count(d, e2, k, x, pivmin);
@@ -308,7 +309,9 @@ __global__ __launch_bounds__(BI_NT) void bisect_kernel(const SectorDesc* __restr
     const double na = L > 0 ? xl : a, nb = L < 32 ? xh : b;
     a = na;
     b = nb;
-    if (b - a <= 2.0 * EPS * fmax(fabs(a), fabs(b)) + pivmin) break;   // warp-uniform
+    // absolute accuracy of a few eps ||T|| (the tridiagonalisation's own error) is all
+    // the selection and sigma = sqrt(lambda) need
+    if (b - a <= tol_abs) break;   // warp-uniform
   }
   if (lane == 0) lam[S.s_off + i] = 0.5 * (a + b);
 }
@@ -409,6 +412,7 @@ __global__ __launch_bounds__(IV_NT) void invit_kernel(const SectorDesc* __restri
     const double lambda = lv[m];
     // factor T - lambda I
     double p = d[0] - lambda, q = k > 1 ? e[0] : 0.0;
+#pragma unroll 4
     for (int i = 0; i < k - 1; ++i) {
       const double ei = e[i], an = d[i + 1] - lambda, en = i + 1 < k - 1 ? e[i + 1] : 0.0;
       const int64_t o = (int64_t)i * kept + m;
@@ -436,6 +440,7 @@ __global__ __launch_bounds__(IV_NT) void invit_kernel(const SectorDesc* __restri
       if (it == 0) {
         for (int i = 0; i < k; ++i) Z[(int64_t)i * kept + m] = start_entry(i, m);
       } else {
+#pragma unroll 4
         for (int i = 0; i < k - 1; ++i) {
           const int64_t o = (int64_t)i * kept + m, o1 = o + kept;
           double bi = Z[o], bn = Z[o1];
@@ -446,6 +451,7 @@ __global__ __launch_bounds__(IV_NT) void invit_kernel(const SectorDesc* __restri
       }
       // back substitution U z = b, then normalise
       double z1 = 0.0, z2 = 0.0, nrm = 0.0;
+#pragma unroll 4
       for (int i = k - 1; i >= 0; --i) {
         const int64_t o = (int64_t)i * kept + m;
         double u0 = U0[o];
@@ -536,7 +542,7 @@ int tridiag_class(int k) { return k <= 64 ? 0 : k <= 160 ? 1 : k <= 320 ? 2 : 3;
 
 cudaError_t launch_tridiag(const SectorDesc* sd_dev, const int* list_dev, const int* class_count,
                            const int* class_kmax, void* gbuf, double* dbuf, double* ebuf,
-                           void* taubuf, cudaStream_t s) {
+                           void* taubuf, const cudaStream_t* streams) {
   // once per process: the largest dynamic shared memory any launch may ask for
   static const cudaError_t attr = cudaFuncSetAttribute(
       tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)td_smem_bytes(eigen_max_k(), 1));
@@ -550,7 +556,7 @@ cudaError_t launch_tridiag(const SectorDesc* sd_dev, const int* list_dev, const 
     cfg.gridDim = dim3(count * cl);
     cfg.blockDim = dim3(TD_NT);
     cfg.dynamicSmemBytes = td_smem_bytes(class_kmax[c], cl);
-    cfg.stream = s;
+    cfg.stream = streams[TD_CLASSES - 1 - c];   // the largest class on the caller's stream
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = cl;
