@@ -31,13 +31,13 @@ namespace cg = cooperative_groups;
 namespace {
 
 constexpr double EPS = 2.220446049250313e-16;
-constexpr int TD_NT = 256;
+constexpr int TD_NT = 512;
 constexpr int TD_CLASSES = 4;   // cluster sizes 1, 2, 4, 8 CTAs per sector, by sector size
 
 // dynamic shared memory of the tridiagonalisation (kmax = largest k of the launch)
 __host__ __device__ inline size_t td_smem_bytes(int kmax, int cl) {
   const int own = kmax / cl + 1;
-  return sizeof(cplx) * ((size_t)5 * kmax + 2 * (size_t)own) + 64 * sizeof(double);
+  return sizeof(cplx) * ((size_t)6 * kmax + 2 * (size_t)own) + 64 * sizeof(double);
 }
 
 __device__ __forceinline__ cplx warp_sum(cplx v) {
@@ -78,7 +78,7 @@ __device__ __forceinline__ cplx cdiv(cplx a, cplx b) {
 //    Two cluster barriers per step; S0 is one warp's work.
 // Every row is read and written by its owner only, so the trailing matrix needs no
 // ordering across CTAs; the vectors travel through distributed shared memory.
-__global__ void __launch_bounds__(TD_NT)
+__global__ void __launch_bounds__(TD_NT, 2)
     tridiag_kernel(const SectorDesc* __restrict__ sd, const int* __restrict__ list, int kmax,
                    cplx* __restrict__ gbuf, double* __restrict__ dbuf, double* __restrict__ ebuf,
                    cplx* __restrict__ taubuf) {
@@ -93,7 +93,8 @@ __global__ void __launch_bounds__(TD_NT)
   cplx* wb = vb + 2 * kmax;
   cplx* vpub = wb + 2 * kmax;          // v_j as published by the owner (index l: column j+1+l)
   cplx* pown = vpub + kmax;            // p_i of the own rows (local index i / TD_CL)
-  double* scal = reinterpret_cast<double*>(pown + 2 * own_cap);   // [0..1] cpart, [2..3] tau, [8..] reduction
+  cplx* stash = pown + 2 * own_cap;    // the owner's next reflector row (row j + 1), updated through step j - 1
+  double* scal = reinterpret_cast<double*>(stash + kmax);   // [0..1] cpart, [2..3] tau, [8..] reduction
   const SectorDesc& S = sd[list[blockIdx.x / TD_CL]];
   const int k = S.k;                   // the same for every CTA of the cluster
   cplx* A = gbuf + S.g_off;
@@ -116,7 +117,9 @@ __global__ void __launch_bounds__(TD_NT)
       double part = 0.0;
       const cplx vj = j > 0 ? vprev[j] : cmake(0.0, 0.0), wj = j > 0 ? wprev[j] : cmake(0.0, 0.0);
       for (int l = j + lane; l < k; l += 32) {
-        cplx a = ldc(row + l);
+        // row j as the previous pass left it (kept in shared memory by this CTA), or the
+        // Gram itself at j = 0
+        cplx a = j > 0 ? stash[l] : ldc(row + l);
         if (j > 0) a = csub(a, cadd(cmulc(vj, wprev[l]), cmulc(wj, vprev[l])));
         if (l == j) {
           dd[j] = a.x;
@@ -164,18 +167,36 @@ __global__ void __launch_bounds__(TD_NT)
       // own rows i > j: first own row, then every TD_CL-th
       const int i0 = j + 1 + ((rank - (j + 1)) % TD_CL + TD_CL) % TD_CL;
       double cpx = 0.0, cpy = 0.0;
-      for (int i = i0 + warp * TD_CL; i < k; i += TD_CL * (TD_NT / 32)) {
+      // two rows per warp in flight (rows i and i + stride), so the loads of one hide
+      // the latency of the other
+      const int stride = TD_CL * (TD_NT / 32);
+      for (int i = i0 + warp * TD_CL; i < k; i += 2 * stride) {
+        const int i2 = i + stride;
+        const bool two = i2 < k;       // warp-uniform
         cplx* row = A + (int64_t)i * k;
+        cplx* row2 = A + (int64_t)(two ? i2 : i) * k;
+        const bool next = i == j + 1;  // the next reflector row: keep it in shared memory
         const cplx vi = j > 0 ? vprev[i] : cmake(0.0, 0.0), wi = j > 0 ? wprev[i] : cmake(0.0, 0.0);
-        cplx acc = cmake(0.0, 0.0);
-#pragma unroll 4
+        const cplx vi2 = (j > 0 && two) ? vprev[i2] : cmake(0.0, 0.0);
+        const cplx wi2 = (j > 0 && two) ? wprev[i2] : cmake(0.0, 0.0);
+        cplx acc = cmake(0.0, 0.0), acc2 = cmake(0.0, 0.0);
+#pragma unroll 2
         for (int l = j + 1 + lane; l < k; l += 32) {
           cplx a = ldc(row + l);
+          cplx a2 = two ? ldc(row2 + l) : cmake(0.0, 0.0);
+          const cplx vc = vcur[l];
           if (j > 0) {
-            a = csub(a, cadd(cmulc(vi, wprev[l]), cmulc(wi, vprev[l])));
+            const cplx vp = vprev[l], wp = wprev[l];
+            a = csub(a, cadd(cmulc(vi, wp), cmulc(wi, vp)));
             stc(row + l, a);
+            if (two) {
+              a2 = csub(a2, cadd(cmulc(vi2, wp), cmulc(wi2, vp)));
+              stc(row2 + l, a2);
+            }
           }
-          cfma(acc, a, vcur[l]);
+          if (next) stash[l] = a;
+          cfma(acc, a, vc);
+          cfma(acc2, a2, vc);
         }
         acc = warp_sum(acc);
         const cplx p = cmul(tau, acc);
@@ -184,6 +205,14 @@ __global__ void __launch_bounds__(TD_NT)
         const cplx cv = ccmul(p, vcur[i]);
         cpx += cv.x;
         cpy += cv.y;
+        if (two) {
+          acc2 = warp_sum(acc2);
+          const cplx p2 = cmul(tau, acc2);
+          if (lane == 0) pown[i2 / TD_CL] = p2;
+          const cplx cv2 = ccmul(p2, vcur[i2]);
+          cpx += cv2.x;
+          cpy += cv2.y;
+        }
       }
       if (lane == 0) {
         scal[8 + 2 * warp] = cpx;
@@ -531,7 +560,7 @@ __global__ __launch_bounds__(BT_NT) void backtransform_kernel(const SectorDesc* 
 }  // namespace
 
 int eigen_max_k() {
-  // shared memory of the tridiagonalisation: (5 k + 2 (k + 1)) x 16 B <= 227 KB with one
+  // shared memory of the tridiagonalisation: (6 k + 2 (k + 1)) x 16 B <= 227 KB with one
   // CTA per sector
   int k = 256;
   while (td_smem_bytes(k + 256, 1) <= 227 * 1024) k += 256;
