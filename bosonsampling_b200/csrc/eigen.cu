@@ -31,7 +31,19 @@ namespace cg = cooperative_groups;
 namespace {
 
 constexpr double EPS = 2.220446049250313e-16;
-constexpr int TD_NT = 512;
+// threads per CTA of the tridiagonalisation and its minimum resident CTAs per SM
+// (compile-time tuning constants)
+// (compile-time tuning constants; measured at chi = 1024 with 16 concurrent updates:
+// 128 x 6 gives 558-564 BS-updates/s, 256 x 3 516-528, 512 x 2 467-501 -- the stage is
+// limited by resident CTA slots shared by the concurrent updates, not by one update's
+// latency)
+#ifndef BSMPO_TD_NT
+#define BSMPO_TD_NT 128
+#endif
+#ifndef BSMPO_TD_MINB
+#define BSMPO_TD_MINB 6
+#endif
+constexpr int TD_NT = BSMPO_TD_NT;
 constexpr int TD_CLASSES = 4;   // cluster sizes 1, 2, 4, 8 CTAs per sector, by sector size
 
 // dynamic shared memory of the tridiagonalisation (kmax = largest k of the launch)
@@ -78,7 +90,7 @@ __device__ __forceinline__ cplx cdiv(cplx a, cplx b) {
 //    Two cluster barriers per step; S0 is one warp's work.
 // Every row is read and written by its owner only, so the trailing matrix needs no
 // ordering across CTAs; the vectors travel through distributed shared memory.
-__global__ void __launch_bounds__(TD_NT, 2)
+__global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
     tridiag_kernel(const SectorDesc* __restrict__ sd, const int* __restrict__ list, int kmax,
                    cplx* __restrict__ gbuf, double* __restrict__ dbuf, double* __restrict__ ebuf,
                    cplx* __restrict__ taubuf) {
@@ -510,7 +522,7 @@ __global__ __launch_bounds__(IV_NT) void invit_kernel(const SectorDesc* __restri
 
 // 3b. y = Q z = H_0 (H_1 (... H_{k-2} z)), one warp per kept vector; lane holds the
 //     entries l = lane (mod 32).  Writes V = y ([k][kept], X = T^H) or Y for the GEMM.
-constexpr int BT_NT = 256;
+constexpr int BT_NT = 128;
 
 template <int NPL>
 __global__ __launch_bounds__(BT_NT) void backtransform_kernel(const SectorDesc* __restrict__ sd,
