@@ -43,9 +43,10 @@ WORKLOADS = {
 WORKLOAD = WORKLOADS["chi1024"]
 METRIC = "BS-updates/s & circuit time at \u03c7=1024 vs plain FP64 GPU path at \u22641e-6 prob err"
 # arithmetic type of each path
-DTYPES = {"fp64": "f64", "fp64-gram": "f64"}
+DTYPES = {"fp64": "f64", "fp64-gram": "f64", "tf32x3": "tf32x3 contractions + f64 Gram/eigen"}
 SVD_KERNELS = {"fp64": "jacobi_gram_kernel + jacobi_apply_kernel (one-sided Jacobi SVD rounds)",
-               "fp64-gram": "zgemm_grouped_kernel (Gram) + tridiag_kernel + bisect_kernel (Gram route SVD)"}
+               "fp64-gram": "zgemm_grouped_kernel (Gram) + tridiag_kernel + bisect_kernel (Gram route SVD)",
+               "tf32x3": "zgemm_grouped_kernel (Gram) + tridiag_kernel + bisect_kernel (Gram route SVD)"}
 
 
 def parse():

@@ -74,6 +74,10 @@ struct bsmpo_ctx {
       env_r, part, outv, dims, nf2, qbuf, qflag, pbuf, pcnt;
   // Gram / eigen route of the sector SVD (precision != BSMPO_PRECISION_FP64)
   DevBuf gbuf, eigd, taub, invsig, escr, swp, zbuf, ybuf;
+  // tensor-core contractions (BSMPO_PRECISION_TF32X3): groups and tensor maps of the
+  // V / W GEMMs, and the pipeline's error word
+  DevBuf tab3, tcerr;
+  HostStage stage3;
   int precision = BSMPO_PRECISION_FP64;
   // the tridiagonalisation's size classes run side by side: three more streams, forked
   // from and joined to `stream` with events
@@ -195,6 +199,9 @@ struct Plan {
   std::vector<GemmGroup> gg;
   std::vector<GemmGroup> ggram;   // Gram G_s = X^H X of every sector (Gram route)
   std::vector<int> tdlist;        // sectors by tridiagonalisation size class (Gram route)
+  std::vector<TcGroup> tcg;       // Theta groups on the tensor cores (TF32X3)
+  std::vector<unsigned char> tcmaps;   // their two tensor maps (Gamma_L, Gamma_R)
+  int tc_tiles = 0;
   int td_count[4] = {0, 0, 0, 0}, td_kmax[4] = {0, 0, 0, 0};
   std::vector<JacobiWork> jw;
   int mix_tiles = 0, gemm_tiles = 0, max_rounds = 0, max_k = 0, max_left_m2 = 0;
@@ -334,6 +341,34 @@ int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
     }
   P.theta_elems = t_off;
   P.gemm_tiles = tiles;
+  // Theta on the tensor cores: one tensor map per site tensor, groups address blocks
+  P.tcg.clear();
+  P.tcmaps.clear();
+  P.tc_tiles = 0;
+  if (h->precision == BSMPO_PRECISION_TF32X3) {
+    const size_t mb = tc_map_bytes();
+    P.tcmaps.assign(2 * mb, 0);
+    const cplx* gl = h->gamma + (size_t)mode * chi2;
+    const cplx* gr = h->gamma + (size_t)(mode + 1) * chi2;
+    if (tc_encode_map(P.tcmaps.data(), gl, h->chi, h->chi, h->chi, 0) != cudaSuccess ||
+        tc_encode_map(P.tcmaps.data() + mb, gr, h->chi, h->chi, h->chi, 2) != cudaSuccess)
+      return fail(h, BSMPO_ECUDA, "tensor map encoding failed");
+    const int tm = tc_tile_m(), tn = tc_tile_n();
+    for (const ThetaDesc& D : P.td) {
+      TcGroup g;
+      std::memset(&g, 0, sizeof(g));
+      g.M = D.nrow; g.N = D.ncol; g.K = D.nk;
+      g.opA = 0; g.mapA = 0; g.mapB = 1;
+      g.a_r0 = D.row0; g.a_c0 = D.k0; g.b_r0 = D.k0; g.b_c0 = D.col0;
+      g.ldc = D.ncol;
+      g.tiles_n = ceil_div(D.ncol, tn);
+      g.tile_start = P.tc_tiles;
+      P.tc_tiles += ceil_div(D.nrow, tm) * g.tiles_n;
+      g.c_off = D.off;
+      g.cs_off = -1;
+      P.tcg.push_back(g);
+    }
+  }
   // Gram groups: G_s = X^H X, X = the first rows_g rows of the sector's Jacobi matrix
   // ([rows_g][k] row-major: T, or T^H when |L| < |R|)
   P.ggram.clear();
@@ -421,7 +456,7 @@ int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
 
 // packs plan tables into the pinned stage and copies them to the device table buffer
 struct TabLayout {
-  size_t tab, tidx, td, sd, pairs, gg, ggram, tdlist, jw, total;
+  size_t tab, tidx, td, sd, pairs, gg, ggram, tdlist, tcmaps, tcg, jw, total;
 };
 
 TabLayout layout_of(const Plan& P) {
@@ -435,6 +470,8 @@ TabLayout layout_of(const Plan& P) {
   L.gg = o; o = align_up(o + P.gg.size() * sizeof(GemmGroup) + 1, 256);
   L.ggram = o; o = align_up(o + P.ggram.size() * sizeof(GemmGroup) + 1, 256);
   L.tdlist = o; o = align_up(o + P.tdlist.size() * sizeof(int) + 1, 256);
+  L.tcmaps = o; o = align_up(o + P.tcmaps.size() + 1, 256);
+  L.tcg = o; o = align_up(o + P.tcg.size() * sizeof(TcGroup) + 1, 256);
   L.jw = o; o = align_up(o + P.jw.size() * sizeof(JacobiWork) + 1, 256);
   L.total = o;
   return L;
@@ -509,6 +546,8 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   put(hs, L.gg, P.gg);
   put(hs, L.ggram, P.ggram);
   put(hs, L.tdlist, P.tdlist);
+  put(hs, L.tcmaps, P.tcmaps);
+  put(hs, L.tcg, P.tcg);
   std::vector<JacobiWork> active(P.jw);
   int gram_ctas = 0, apply_ctas = 0, slots = 0;
   jacobi_launch_list(active, &gram_ctas, &apply_ctas, &slots);
@@ -523,6 +562,15 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   const GemmGroup* gg_d = reinterpret_cast<const GemmGroup*>(dt + L.gg);
   const GemmGroup* ggram_d = reinterpret_cast<const GemmGroup*>(dt + L.ggram);
   const int* tdlist_d = reinterpret_cast<const int*>(dt + L.tdlist);
+  const bool tc = h->precision == BSMPO_PRECISION_TF32X3;
+  int* tcerr_d = nullptr;
+  if (tc) {
+    if (!h->tcerr.p) {
+      if ((rc = grow(h, h->tcerr, sizeof(int)))) return rc;
+      CK(h, cudaMemsetAsync(h->tcerr.p, 0, sizeof(int), st));
+    }
+    tcerr_d = reinterpret_cast<int*>(h->tcerr.p);
+  }
   // The Gram route drops singular values below ~2e-6 of a sector's largest.  Where the
   // update does not truncate to chi that is pure loss (W = V^H C carries them through
   // 1 / Lambda_R), so such updates take the exact Jacobi SVD: up front when the
@@ -543,8 +591,12 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
 
   if ((rc = clk.mark(0))) return rc;
   // 1. Theta_q = Glc[a, q] Gcr[q, b] for every valid triple
-  CKL(h, launch_zgemm_grouped(h->gamma, h->gamma, h->theta.p, nullptr, gg_d, (int)P.gg.size(),
-                              P.gemm_tiles, st));
+  if (tc)
+    CKL(h, launch_tc_zgemm(reinterpret_cast<const TcGroup*>(dt + L.tcg), (int)P.tcg.size(), P.tc_tiles,
+                           dt + L.tcmaps, h->theta.p, nullptr, tcerr_d, st));
+  else
+    CKL(h, launch_zgemm_grouped(h->gamma, h->gamma, h->theta.p, nullptr, gg_d, (int)P.gg.size(),
+                                P.gemm_tiles, st));
   if ((rc = clk.mark(1))) return rc;
   // 2. identity rows of [T^H; I] and the gate mix
   if (!gram) CKL(h, launch_identity_rows(sd_d, ns, P.max_left_m2, h->abuf.p, st));
@@ -725,7 +777,11 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
                        reinterpret_cast<double*>(h->keys.p), h->cutoff, chi, kept_d, trunc_d, st));
   CK(h, cudaMemcpyAsync(hk, kept_d, (size_t)(ns + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(h, cudaMemcpyAsync(htw, trunc_d, sizeof(double), cudaMemcpyDeviceToHost, st));
+  int* htc = reinterpret_cast<int*>(static_cast<char*>(h->hres.p) + 1000);
+  if (tc) CK(h, cudaMemcpyAsync(htc, tcerr_d, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(h, host_wait(h));
+  if (tc && *htc != 0)
+    return fail(h, BSMPO_ECUDA, "tensor-core GEMM: a pipeline wait expired (error word set)");
   total_kept = hk[ns];
   if (gram && total_kept < chi && h->cutoff == 0.0 && h->gram_policy >= 1) {
     // not truncated to chi: redo the SVD exactly (the Gram matrix and the eigen buffers
@@ -811,14 +867,81 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
                         reinterpret_cast<double*>(h->zbuf.p), h->gbuf.p, h->taub.p, h->vbuf.p, h->ybuf.p,
                         st));
     h->launches += 2;
-    if (!vg.empty())
+    if (!vg.empty() && !tc)
       CKL(h, launch_zgemm_grouped(h->abuf.p, h->ybuf.p, h->vbuf.p, reinterpret_cast<double*>(h->invsig.p),
                                   vg_d, (int)vg.size(), vtiles, st));
   } else {
     CKL(h, launch_extract_v(sd_d, ns, max_vm, h->abuf.p, reinterpret_cast<double*>(h->sig.p),
                             reinterpret_cast<int*>(h->perm.p), h->vbuf.p, st));
   }
-  CKL(h, launch_zgemm_grouped(h->vbuf.p, h->cbuf.p, h->wbuf.p, nullptr, wg_d, (int)wg.size(), wtiles, st));
+  if (tc) {
+    // V = T Y diag(1/sigma) and W = V^H C on the tensor cores: two tensor maps per group
+    const size_t mb = tc_map_bytes();
+    std::vector<unsigned char> maps;
+    std::vector<TcGroup> tv, tw;
+    int tv_tiles = 0, tw_tiles = 0;
+    const int tm = tc_tile_m(), tn = tc_tile_n();
+    bool enc_ok = true;
+    auto add_map = [&](const void* base, int rows, int cols, int ld, int kind) -> int {
+      const int idx = (int)(maps.size() / mb);
+      maps.resize(maps.size() + mb);
+      if (tc_encode_map(maps.data() + (size_t)idx * mb, base, rows, cols, ld, kind) != cudaSuccess) enc_ok = false;
+      return idx;
+    };
+    const cplx* A0 = reinterpret_cast<const cplx*>(h->abuf.p);
+    const cplx* Y0 = reinterpret_cast<const cplx*>(h->ybuf.p);
+    const cplx* V0 = reinterpret_cast<const cplx*>(h->vbuf.p);
+    const cplx* C0 = reinterpret_cast<const cplx*>(h->cbuf.p);
+    for (int s = 0; s < ns; ++s) {
+      const SectorDesc& S = P.sd[s];
+      const int kp = hk[s];
+      if (kp == 0) continue;
+      if (gram && !S.left) {
+        TcGroup g;
+        std::memset(&g, 0, sizeof(g));
+        g.M = S.m; g.N = kp; g.K = S.k; g.opA = 0;
+        g.mapA = add_map(A0 + S.a_off, S.m, S.k, S.k, 0);
+        g.mapB = add_map(Y0 + S.y_off, S.k, kp, kp, 2);
+        g.ldc = kp;
+        g.tiles_n = ceil_div(kp, tn);
+        g.tile_start = tv_tiles;
+        tv_tiles += ceil_div(S.m, tm) * g.tiles_n;
+        g.c_off = S.v_off;
+        g.cs_off = S.s_off;
+        tv.push_back(g);
+      }
+      TcGroup g;
+      std::memset(&g, 0, sizeof(g));
+      g.M = kp; g.N = S.n; g.K = S.m; g.opA = 1;
+      g.mapA = add_map(V0 + S.v_off, S.m, kp, kp, 1);
+      g.mapB = add_map(C0 + S.c_off, S.m, S.n, S.n, 2);
+      g.ldc = S.n;
+      g.tiles_n = ceil_div(S.n, tn);
+      g.tile_start = tw_tiles;
+      tw_tiles += ceil_div(kp, tm) * g.tiles_n;
+      g.c_off = S.w_off;
+      g.cs_off = -1;
+      tw.push_back(g);
+    }
+    if (!enc_ok) return fail(h, BSMPO_ECUDA, "tensor map encoding failed");
+    const size_t o_tv = align_up(maps.size(), 256);
+    const size_t o_tw = align_up(o_tv + tv.size() * sizeof(TcGroup) + 1, 256);
+    const size_t total = align_up(o_tw + tw.size() * sizeof(TcGroup) + 1, 256);
+    if ((rc = grow(h, h->tab3, total))) return rc;
+    if ((rc = grow_host(h, h->stage3, total))) return rc;
+    std::memcpy(h->stage3.p, maps.data(), maps.size());
+    put(h->stage3.p, o_tv, tv);
+    put(h->stage3.p, o_tw, tw);
+    CK(h, cudaMemcpyAsync(h->tab3.p, h->stage3.p, total, cudaMemcpyHostToDevice, st));
+    const char* t3 = static_cast<const char*>(h->tab3.p);
+    if (!tv.empty())
+      CKL(h, launch_tc_zgemm(reinterpret_cast<const TcGroup*>(t3 + o_tv), (int)tv.size(), tv_tiles, t3,
+                             h->vbuf.p, reinterpret_cast<double*>(h->invsig.p), tcerr_d, st));
+    CKL(h, launch_tc_zgemm(reinterpret_cast<const TcGroup*>(t3 + o_tw), (int)tw.size(), tw_tiles, t3,
+                           h->wbuf.p, nullptr, tcerr_d, st));
+  } else {
+    CKL(h, launch_zgemm_grouped(h->vbuf.p, h->cbuf.p, h->wbuf.p, nullptr, wg_d, (int)wg.size(), wtiles, st));
+  }
   if ((rc = clk.mark(5))) return rc;
   // 6. scatter into Gamma[mode], Gamma[mode+1], Lambda / charge of bond mode+1
   CKL(h, launch_scatter(tab_d, sd_d, ns, total_kept, chi, h->charge + (size_t)mode * chi * 2,
@@ -881,11 +1004,11 @@ void free_workspaces(bsmpo_ctx* h) {
                     &h->perm, &h->tab, &h->tab2, &h->rot, &h->kept, &h->u3, &h->m4,
                     &h->env_l, &h->env_r, &h->part, &h->outv, &h->dims, &h->nf2, &h->qbuf,
                     &h->qflag, &h->pbuf, &h->pcnt, &h->gbuf, &h->eigd, &h->taub, &h->invsig,
-                    &h->escr, &h->swp, &h->zbuf, &h->ybuf};
+                    &h->escr, &h->swp, &h->zbuf, &h->ybuf, &h->tab3, &h->tcerr};
   for (DevBuf* b : bufs)
     if (b->p) cudaFreeAsync(b->p, h->stream);
   cudaStreamSynchronize(h->stream);
-  HostStage* hs[] = {&h->stage, &h->stage2, &h->hres};
+  HostStage* hs[] = {&h->stage, &h->stage2, &h->stage3, &h->hres};
   for (HostStage* b : hs)
     if (b->p) cudaFreeHost(b->p);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -1130,6 +1253,43 @@ int bsmpo_contract_sector(int d, int cc0, int cc1, const void* u, const void* gl
   return BSMPO_OK;
 }
 
+int bsmpo_zgemm_tf32x3(int M, int N, int K, const void* a, int lda, int opA, const void* b, int ldb,
+                       void* c, int ldc, void* stream) {
+  if (M < 0 || N < 0 || K < 1 || !a || !b || !c || (opA != 0 && opA != 1) || ldb < N || ldc < N ||
+      lda < (opA ? M : K))
+    return fail(nullptr, BSMPO_EINVAL, "bsmpo_zgemm_tf32x3: bad argument");
+  if (M == 0 || N == 0) return BSMPO_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t mb = tc_map_bytes();
+  const size_t o_g = align_up(2 * mb, 256), o_err = o_g + 256, total = o_err + 256;
+  std::vector<unsigned char> host(total, 0);
+  if (tc_encode_map(host.data(), a, opA ? K : M, opA ? M : K, lda, opA ? 1 : 0) != cudaSuccess ||
+      tc_encode_map(host.data() + mb, b, K, N, ldb, 2) != cudaSuccess)
+    return fail(nullptr, BSMPO_ECUDA, "bsmpo_zgemm_tf32x3: tensor map encoding failed");
+  TcGroup g;
+  std::memset(&g, 0, sizeof(g));
+  g.M = M; g.N = N; g.K = K; g.opA = opA; g.mapA = 0; g.mapB = 1;
+  g.ldc = ldc;
+  g.tiles_n = ceil_div(N, tc_tile_n());
+  g.tile_start = 0;
+  g.cs_off = -1;
+  std::memcpy(host.data() + o_g, &g, sizeof(g));
+  void* dev = nullptr;
+  cudaError_t e = cudaMallocAsync(&dev, total, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice, st);
+  int herr = 0;
+  char* dc = static_cast<char*>(dev);
+  if (e == cudaSuccess)
+    e = launch_tc_zgemm(reinterpret_cast<const TcGroup*>(dc + o_g), 1, ceil_div(M, tc_tile_m()) * g.tiles_n, dc, c,
+                        nullptr, reinterpret_cast<int*>(dc + o_err), st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, dc + o_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (dev) cudaFreeAsync(dev, st);
+  if (e != cudaSuccess) return fail(nullptr, BSMPO_ECUDA, std::string("bsmpo_zgemm_tf32x3: ") + cudaGetErrorString(e));
+  if (herr) return fail(nullptr, BSMPO_ECUDA, "bsmpo_zgemm_tf32x3: a pipeline wait expired");
+  return BSMPO_OK;
+}
+
 int bsmpo_create(int n, int d, int chi, int flags, bsmpo_ctx** out) {
   if (!out) return fail(nullptr, BSMPO_EINVAL, "null output handle");
   *out = nullptr;
@@ -1200,7 +1360,8 @@ int bsmpo_set_stream(bsmpo_ctx* h, void* stream) {
 
 int bsmpo_set_precision(bsmpo_ctx* h, int precision) {
   if (!h) return fail(nullptr, BSMPO_EINVAL, "null handle");
-  if (precision != BSMPO_PRECISION_FP64 && precision != BSMPO_PRECISION_FP64_GRAM)
+  if (precision != BSMPO_PRECISION_FP64 && precision != BSMPO_PRECISION_FP64_GRAM &&
+      precision != BSMPO_PRECISION_TF32X3)
     return fail(h, BSMPO_EINVAL, "unknown precision mode " + std::to_string(precision));
   h->precision = precision;
   return BSMPO_OK;

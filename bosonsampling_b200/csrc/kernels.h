@@ -181,6 +181,33 @@ cudaError_t launch_eigvec(const SectorDesc* sd_dev, int n_sectors, int kmax, int
                           double* scratch, unsigned char* swp, double* zbuf, const void* gbuf,
                           const void* taubuf, void* vbuf, void* ybuf, cudaStream_t s);
 
+// ---------------------------------------------------------------- tcgemm.cu
+// One group of the tensor-core (tcgen05, 3 x TF32) grouped complex GEMM:
+//   C[c_off + m ldc + n] = sum_k op(A)[m][k] B[k][n] (x scale[cs_off + n])
+// A and B are read through TMA tensor maps (index mapA / mapB into the launch's map
+// array, FP64 views of complex matrices): op(A) = A ([m][k] at row a_r0 + m, column
+// a_c0 + k; opA 0) or A^H (A stored [k][m] at row a_r0 + k, column a_c0 + m; opA 1);
+// B [k][n] at row b_r0 + k, column b_c0 + n.  Offsets in complex elements.
+struct TcGroup {
+  int M, N, K;
+  int opA;
+  int tiles_n, tile_start;
+  int mapA, mapB;
+  int a_r0, a_c0, b_r0, b_c0;
+  int ldc, pad_;
+  int64_t c_off, cs_off;
+};
+int tc_tile_m();
+int tc_tile_n();
+size_t tc_map_bytes();
+// Encodes a tensor map (tc_map_bytes() bytes at map_out) of the complex matrix at base
+// (rows x cols, leading dimension ld, complex elements) with the box of operand `kind`:
+// 0 = A [m][k], 1 = A stored [k][m], 2 = B [k][n].
+cudaError_t tc_encode_map(void* map_out, const void* base, int rows, int cols, int ld, int kind);
+// err: device int, set to nonzero if a pipeline wait of the kernel expired.
+cudaError_t launch_tc_zgemm(const TcGroup* groups_dev, int n_groups, int total_tiles, const void* maps_dev,
+                            void* c, const double* scale, int* err, cudaStream_t s);
+
 // ---------------------------------------------------------------- contract.cu
 // Standalone sector contraction with per-element charges (the update_MPO drop-in).
 cudaError_t launch_contract_sector(int d, int cc0, int cc1, const void* u, const void* glc,

@@ -68,11 +68,12 @@ class MPOSimulator:
     def set_cutoff(self, cutoff):
         self._chk(self.L.bsmpo_set_cutoff(self.h, float(cutoff)))
 
-    PRECISIONS = {"fp64": 0, "fp64-gram": 1}
+    PRECISIONS = {"fp64": 0, "fp64-gram": 1, "tf32x3": 2}
 
     def set_precision(self, precision):
-        """Sector SVD / contraction mode: 'fp64' (Jacobi, the plain path) or 'fp64-gram'
-        (FP64 Gram + Hermitian eigenproblem)."""
+        """Sector SVD / contraction mode: 'fp64' (Jacobi, the plain path), 'fp64-gram'
+        (FP64 Gram + Hermitian eigenproblem) or 'tf32x3' (the Gram route with the
+        contractions on the tensor cores, 3 x TF32 split products)."""
         self._chk(self.L.bsmpo_set_precision(self.h, self.PRECISIONS[precision]))
 
     def set_workers(self, n_workers):

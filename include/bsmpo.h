@@ -74,6 +74,16 @@ int bsmpo_contract_sector(int d, int cc0, int cc1, const void* u,
                           const int* cl, const int* cc, const int* cr,
                           int len_l, int len_c, int len_r, void* c, void* stream);
 
+/* Complex GEMM on the tensor cores with three TF32 split products (hi*hi + hi*lo +
+ * lo*hi, FP32 accumulation): C[m][n] = sum_k op(A)[m][k] B[k][n], the contraction
+ * primitive of BSMPO_PRECISION_TF32X3 (the reference's update_MPO_kernel.cu GEMM,
+ * src/update_MPO_kernel.cu:193-733, computes in FP32 SIMT).  Device complex128
+ * row-major matrices: op(A) = A [M][K] (opA 0, lda >= K) or A^H with A stored [K][M]
+ * (opA 1, lda >= M); B [K][N]; C [M][N] is overwritten.  Synchronises `stream`; error
+ * about 2^-21 relative per product. */
+int bsmpo_zgemm_tf32x3(int M, int N, int K, const void* a, int lda, int opA, const void* b, int ldb,
+                       void* c, int ldc, void* stream);
+
 /* Create a handle for an n-mode chain with local cutoff d and bond dimension chi.
  * Allocates the device state (n chi^2 complex128) and workspaces on the current
  * device.  flags: reserved, pass 0. */
@@ -102,6 +112,12 @@ int bsmpo_set_stream(bsmpo_ctx* h, void* stream);
  *                              bond holds fewer than chi vectors. */
 #define BSMPO_PRECISION_FP64 0
 #define BSMPO_PRECISION_FP64_GRAM 1
+/*   BSMPO_PRECISION_TF32X3     the Gram route with the contractions (the Theta block
+ *                              products, V = T Y / sigma, W = V^H C) on the tensor cores
+ *                              (tcgen05): 3 x TF32 split products, FP32 accumulation;
+ *                              the Gram, the eigenproblem, Lambda and the observables
+ *                              stay FP64. */
+#define BSMPO_PRECISION_TF32X3 2
 int bsmpo_set_precision(bsmpo_ctx* h, int precision);
 
 /* Relative singular-value cutoff: a singular value s is kept only if
