@@ -867,7 +867,10 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
                         reinterpret_cast<double*>(h->zbuf.p), h->gbuf.p, h->taub.p, h->vbuf.p, h->ybuf.p,
                         st));
     h->launches += 2;
-    if (!vg.empty() && !tc)
+    // V = T Y diag(1/sigma) stays FP64: it divides by sigma (down to ~3e-3 of the largest
+    // at the cut), which would magnify a TF32 error into V's orthogonality, and a
+    // non-orthonormal V leaks into W = V^H C at the scale of C
+    if (!vg.empty())
       CKL(h, launch_zgemm_grouped(h->abuf.p, h->ybuf.p, h->vbuf.p, reinterpret_cast<double*>(h->invsig.p),
                                   vg_d, (int)vg.size(), vtiles, st));
   } else {
@@ -875,11 +878,11 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
                             reinterpret_cast<int*>(h->perm.p), h->vbuf.p, st));
   }
   if (tc) {
-    // V = T Y diag(1/sigma) and W = V^H C on the tensor cores: two tensor maps per group
+    // W = V^H C on the tensor cores: two tensor maps per group
     const size_t mb = tc_map_bytes();
     std::vector<unsigned char> maps;
-    std::vector<TcGroup> tv, tw;
-    int tv_tiles = 0, tw_tiles = 0;
+    std::vector<TcGroup> tw;
+    int tw_tiles = 0;
     const int tm = tc_tile_m(), tn = tc_tile_n();
     bool enc_ok = true;
     auto add_map = [&](const void* base, int rows, int cols, int ld, int kind) -> int {
@@ -888,28 +891,12 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
       if (tc_encode_map(maps.data() + (size_t)idx * mb, base, rows, cols, ld, kind) != cudaSuccess) enc_ok = false;
       return idx;
     };
-    const cplx* A0 = reinterpret_cast<const cplx*>(h->abuf.p);
-    const cplx* Y0 = reinterpret_cast<const cplx*>(h->ybuf.p);
     const cplx* V0 = reinterpret_cast<const cplx*>(h->vbuf.p);
     const cplx* C0 = reinterpret_cast<const cplx*>(h->cbuf.p);
     for (int s = 0; s < ns; ++s) {
       const SectorDesc& S = P.sd[s];
       const int kp = hk[s];
       if (kp == 0) continue;
-      if (gram && !S.left) {
-        TcGroup g;
-        std::memset(&g, 0, sizeof(g));
-        g.M = S.m; g.N = kp; g.K = S.k; g.opA = 0;
-        g.mapA = add_map(A0 + S.a_off, S.m, S.k, S.k, 0);
-        g.mapB = add_map(Y0 + S.y_off, S.k, kp, kp, 2);
-        g.ldc = kp;
-        g.tiles_n = ceil_div(kp, tn);
-        g.tile_start = tv_tiles;
-        tv_tiles += ceil_div(S.m, tm) * g.tiles_n;
-        g.c_off = S.v_off;
-        g.cs_off = S.s_off;
-        tv.push_back(g);
-      }
       TcGroup g;
       std::memset(&g, 0, sizeof(g));
       g.M = kp; g.N = S.n; g.K = S.m; g.opA = 1;
@@ -924,19 +911,14 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
       tw.push_back(g);
     }
     if (!enc_ok) return fail(h, BSMPO_ECUDA, "tensor map encoding failed");
-    const size_t o_tv = align_up(maps.size(), 256);
-    const size_t o_tw = align_up(o_tv + tv.size() * sizeof(TcGroup) + 1, 256);
+    const size_t o_tw = align_up(maps.size(), 256);
     const size_t total = align_up(o_tw + tw.size() * sizeof(TcGroup) + 1, 256);
     if ((rc = grow(h, h->tab3, total))) return rc;
     if ((rc = grow_host(h, h->stage3, total))) return rc;
     std::memcpy(h->stage3.p, maps.data(), maps.size());
-    put(h->stage3.p, o_tv, tv);
     put(h->stage3.p, o_tw, tw);
     CK(h, cudaMemcpyAsync(h->tab3.p, h->stage3.p, total, cudaMemcpyHostToDevice, st));
     const char* t3 = static_cast<const char*>(h->tab3.p);
-    if (!tv.empty())
-      CKL(h, launch_tc_zgemm(reinterpret_cast<const TcGroup*>(t3 + o_tv), (int)tv.size(), tv_tiles, t3,
-                             h->vbuf.p, reinterpret_cast<double*>(h->invsig.p), tcerr_d, st));
     CKL(h, launch_tc_zgemm(reinterpret_cast<const TcGroup*>(t3 + o_tw), (int)tw.size(), tw_tiles, t3,
                            h->wbuf.p, nullptr, tcerr_d, st));
   } else {

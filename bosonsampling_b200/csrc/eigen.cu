@@ -32,7 +32,6 @@ namespace {
 
 constexpr double EPS = 2.220446049250313e-16;
 // threads per CTA of the tridiagonalisation and its minimum resident CTAs per SM
-// (compile-time tuning constants)
 // (compile-time tuning constants; measured at chi = 1024 with 16 concurrent updates:
 // 128 x 6 gives 558-564 BS-updates/s, 256 x 3 516-528, 512 x 2 467-501 -- the stage is
 // limited by resident CTA slots shared by the concurrent updates, not by one update's

@@ -113,10 +113,10 @@ int bsmpo_set_stream(bsmpo_ctx* h, void* stream);
 #define BSMPO_PRECISION_FP64 0
 #define BSMPO_PRECISION_FP64_GRAM 1
 /*   BSMPO_PRECISION_TF32X3     the Gram route with the contractions (the Theta block
- *                              products, V = T Y / sigma, W = V^H C) on the tensor cores
- *                              (tcgen05): 3 x TF32 split products, FP32 accumulation;
- *                              the Gram, the eigenproblem, Lambda and the observables
- *                              stay FP64. */
+ *                              products and W = V^H C) on the tensor cores (tcgen05):
+ *                              3 x TF32 split products, FP32 accumulation; the Gram,
+ *                              the eigenproblem, V = T Y / sigma, Lambda and the
+ *                              observables stay FP64. */
 #define BSMPO_PRECISION_TF32X3 2
 int bsmpo_set_precision(bsmpo_ctx* h, int precision);
 
