@@ -87,6 +87,9 @@ struct bsmpo_ctx {
   // cannot exceed chi; 1 also after a selection that keeps fewer than chi; 2 also where
   // the centre bond holds fewer than chi vectors
   int gram_policy = 0;
+  // which contractions of BSMPO_PRECISION_TF32X3 go on the tensor cores (BSMPO_TC_MASK,
+  // read at create): bit 0 the Theta block products, bit 1 W = V^H C; the others FP64
+  int tc_mask = 3;
   HostStage stage, stage2, hres;
   // last update diagnostics (host)
   std::vector<int> last_cc, last_shape, last_kept, last_k;
@@ -345,7 +348,7 @@ int make_plan(bsmpo_ctx* h, int mode, Plan& P) {
   P.tcg.clear();
   P.tcmaps.clear();
   P.tc_tiles = 0;
-  if (h->precision == BSMPO_PRECISION_TF32X3) {
+  if (h->precision == BSMPO_PRECISION_TF32X3 && (h->tc_mask & 1)) {
     const size_t mb = tc_map_bytes();
     P.tcmaps.assign(2 * mb, 0);
     const cplx* gl = h->gamma + (size_t)mode * chi2;
@@ -563,6 +566,7 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   const GemmGroup* ggram_d = reinterpret_cast<const GemmGroup*>(dt + L.ggram);
   const int* tdlist_d = reinterpret_cast<const int*>(dt + L.tdlist);
   const bool tc = h->precision == BSMPO_PRECISION_TF32X3;
+  const bool tc_theta = tc && (h->tc_mask & 1), tc_w = tc && (h->tc_mask & 2);
   int* tcerr_d = nullptr;
   if (tc) {
     if (!h->tcerr.p) {
@@ -591,7 +595,7 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
 
   if ((rc = clk.mark(0))) return rc;
   // 1. Theta_q = Glc[a, q] Gcr[q, b] for every valid triple
-  if (tc)
+  if (tc_theta)
     CKL(h, launch_tc_zgemm(reinterpret_cast<const TcGroup*>(dt + L.tcg), (int)P.tcg.size(), P.tc_tiles,
                            dt + L.tcmaps, h->theta.p, nullptr, tcerr_d, st));
   else
@@ -877,7 +881,7 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
     CKL(h, launch_extract_v(sd_d, ns, max_vm, h->abuf.p, reinterpret_cast<double*>(h->sig.p),
                             reinterpret_cast<int*>(h->perm.p), h->vbuf.p, st));
   }
-  if (tc) {
+  if (tc_w) {
     // W = V^H C on the tensor cores: two tensor maps per group
     const size_t mb = tc_map_bytes();
     std::vector<unsigned char> maps;
@@ -1051,6 +1055,7 @@ int run_mesh_concurrent(bsmpo_ctx* h, int n_bs, const int* modes, const cplx* u3
     w->cutoff = h->cutoff;
     w->precision = h->precision;
     w->gram_policy = h->gram_policy;
+    w->tc_mask = h->tc_mask;
     w->jac_rows = h->jac_rows;
     w->timing = h->timing;
     if (w->timing && !w->ev0) {
@@ -1307,6 +1312,8 @@ int bsmpo_create(int n, int d, int chi, int flags, bsmpo_ctx** out) {
   h->profile = prof && prof[0] == '1';
   const char* jr = std::getenv("BSMPO_JACOBI_ROWS");
   if (jr && std::atoi(jr) >= 16) h->jac_rows = std::atoi(jr);
+  const char* tm = std::getenv("BSMPO_TC_MASK");
+  if (tm && tm[0] >= '0' && tm[0] <= '3') h->tc_mask = tm[0] - '0';
   const char* gp = std::getenv("BSMPO_GRAM_POLICY");
   if (gp && gp[0] >= '0' && gp[0] <= '2') h->gram_policy = gp[0] - '0';
   const char* nwk = std::getenv("BSMPO_WORKERS");
