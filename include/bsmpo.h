@@ -112,11 +112,16 @@ int bsmpo_set_stream(bsmpo_ctx* h, void* stream);
  *                              bond holds fewer than chi vectors. */
 #define BSMPO_PRECISION_FP64 0
 #define BSMPO_PRECISION_FP64_GRAM 1
-/*   BSMPO_PRECISION_TF32X3     the Gram route with the contractions (the Theta block
- *                              products and W = V^H C) on the tensor cores (tcgen05):
- *                              3 x TF32 split products, FP32 accumulation; the Gram,
- *                              the eigenproblem, V = T Y / sigma, Lambda and the
- *                              observables stay FP64. */
+/*   BSMPO_PRECISION_TF32X3     the Gram route with the two-site contraction (the Theta
+ *                              block products) on the tensor cores (tcgen05): 3 x TF32
+ *                              split products, FP32 accumulation; the Gram, the
+ *                              eigenproblem, V = T Y / sigma, W = V^H C, Lambda and the
+ *                              observables stay FP64 (BSMPO_TC_MASK=3 in the environment
+ *                              at create also puts W on the tensor cores).  Measured
+ *                              marginal error against FP64: ~1e-5 (N=16, chi=64) to
+ *                              ~1e-4 (N=32, chi=256) of the trace -- the FP32
+ *                              accumulation of the split products bounds it, so this
+ *                              mode does not reach 1e-6 on these circuits. */
 #define BSMPO_PRECISION_TF32X3 2
 int bsmpo_set_precision(bsmpo_ctx* h, int precision);
 
