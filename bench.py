@@ -65,6 +65,9 @@ def parse():
                    help="the measured path: fp64-gram (Gram matrix + Hermitian eigenproblem, the "
                         "default) or fp64 (the plain path: one-sided Jacobi)")
     p.add_argument("--workers", type=int, default=0, help="concurrent updates (0: 16, or 8 for fp64)")
+    p.add_argument("--also", default="tf32x3",
+                   help="comma-separated further precision forms timed on the same layers and "
+                        "checked over the whole circuit ('' for none)")
     p.add_argument("--no-plain", action="store_true",
                    help="skip the plain FP64 path (the metric's denominator) and the error against it")
     p.add_argument("--bs-slice", default=None,
@@ -199,6 +202,27 @@ def layers_of(bs):
     return out
 
 
+def measure_hbm_peak(torch):
+    """Copy bandwidth (torch copy of 1 GiB, read + write counted, best of 10): the HBM
+    roofline measured in the same run."""
+    n = 1 << 30
+    a = torch.empty(n, dtype=torch.uint8, device="cuda")
+    b = torch.empty_like(a)
+    b.copy_(a)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(10):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b.copy_(a)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n / best / 1e9
+
+
 def measure_fp64_peak(torch):
     """DGEMM TFLOP/s (torch.matmul float64 8192^3, best of 5) -- the FP64 roofline."""
     n = 8192
@@ -304,6 +328,37 @@ def run_reference(args):
     return 0
 
 
+# DRAM bytes (read + write) of one tridiag_kernel launch of the largest size class
+# (8-CTA clusters, the biggest sector of a centre update at chi = 1024), from the ncu
+# capture summarised under profiles/ (cold cache)
+TRIDIAG_TRAFFIC = None
+
+
+def roofline(args, mine, kernel, fp64_peak, hbm_peak):
+    """The dominant kernel's roofline.  Gram route: the Householder tridiagonalisation
+    (tridiag_kernel, 66-71% of the update's kernel time), whose fused passes stream the
+    trailing matrix once per step (read + write, 32 B per complex entry): achieved
+    bytes / device time of the phase, one worker, against the copy bandwidth measured in
+    this run.  Plain path: the Jacobi rounds' FP64 flops against measured DGEMM."""
+    if kernel is not None and kernel["ms"] > 0:
+        achieved = kernel["bytes"] / (kernel["ms"] / 1e3) / 1e9
+        return {"kernel": "tridiag_kernel (Householder tridiagonalisation, four forked size-class launches)",
+                "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak if hbm_peak else None,
+                "peak_source": "copy bandwidth measured in this run (torch copy of 1 GiB, best of 10)",
+                "achieved_over": "the phase's device time (CUDA events), one worker, one layer (%d phases)"
+                                 % kernel["phases"],
+                "bytes": kernel["bytes"], "ms": kernel["ms"],
+                "flops_tflops": kernel["flops"] / (kernel["ms"] / 1e3) / 1e12,
+                "traffic": TRIDIAG_TRAFFIC, "traffic_unit": "bytes per launch (largest class)"}
+    achieved = mine["svd_flops"] / mine["seconds"] / 1e12 if mine["seconds"] > 0 else None
+    return {"kernel": SVD_KERNELS[args.precision], "bound": "tensor", "achieved": achieved, "peak": fp64_peak,
+            "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if achieved and fp64_peak else None,
+            "peak_source": "FP64 DGEMM measured in this run (torch.matmul 8192^3, best of 5)",
+            "achieved_over": "timed region (device time); the SVD phases of concurrent updates overlap",
+            "traffic": None}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -407,8 +462,29 @@ def main():
     if args.precision != "fp64" and not args.no_plain:
         plain = timed_layers("fp64", 8)
         plain["value"] = replica_rate(n_bs, world, plain["seconds"])
+    extras = {}
+    also = [x for x in args.also.split(",") if x and x != args.precision]
+    for form in also:
+        r = timed_layers(form, workers)
+        r["value"] = replica_rate(n_bs, world, r["seconds"])
+        extras[form] = r
     if world > 1:
         dist.barrier()
+
+    # ---- the dominant kernel alone: one worker, one layer, the tridiagonalisation phase
+    # timed with CUDA events around its launches (the Gram route's forked size classes)
+    kernel = None
+    if args.precision != "fp64":
+        sim.load(g0, l0, c0)
+        sim.set_precision(args.precision)
+        sim.set_workers(1)
+        run_layers(sim, args.start_layer, args.warmup)
+        sim.set_timing(True)
+        run_layers(sim, first, 1, partial=True)
+        torch.cuda.synchronize()
+        td_ms, td_bytes, td_flops, td_phases = sim.tridiag_timing()
+        sim.set_timing(False)
+        kernel = {"ms": td_ms, "bytes": td_bytes, "flops": td_flops, "phases": td_phases}
 
     # ---- end to end through the public API with host buffers, over the same K layers: per
     # step (layer) the state is copied host -> device and loaded, the layer runs, the state
@@ -449,7 +525,8 @@ def main():
     circuit = None
     if not args.no_circuit and not args.bs_slice:
         runs = {}
-        for prec in ([args.precision] + (["fp64"] if args.precision != "fp64" and not args.no_plain else [])):
+        for prec in ([args.precision] + also +
+                     (["fp64"] if args.precision != "fp64" and not args.no_plain else [])):
             with engine.MPOSimulator(w["n"], w["d"], w["chi"]) as full:
                 full.set_precision(prec)
                 full.set_workers(workers if prec == args.precision else 8)
@@ -477,10 +554,16 @@ def main():
             circuit["prob_err_vs_fp64"] = float(np.abs(P_c - P_p).max() / abs(trace_p))
             circuit["trace_err_vs_fp64"] = float(abs(trace_c - trace_p) / abs(trace_p))
             circuit["truncation_weight_err_vs_fp64"] = float(np.abs(tw_c - tw_p).max())
+            for form in also:
+                t_f, trace_f, P_f, _ = runs[form]
+                extras[form]["circuit"] = {"seconds": round(t_f, 3),
+                                           "value": replica_rate(len(bs), world, t_f),
+                                           "prob_err_vs_fp64": float(np.abs(P_f - P_p).max() / abs(trace_p))}
 
     # ---- roofline of the dominant phase: the SVD step (Jacobi rounds, or the Gram GEMM,
     # Householder reduction and bisection of the Gram route), FP64 against measured DGEMM
     fp64_peak = measure_fp64_peak(torch) if rank == 0 else None
+    hbm_peak = measure_hbm_peak(torch) if rank == 0 else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import mpo as _mpo
@@ -517,13 +600,12 @@ def main():
                     "covers": "K steps, each: state host->device, load, one layer, store, device->host, trace"},
             "gpu_launches": int(mine["launches"]),
             "svd_routes": mine["routes"],
-            "roofline": {"kernel": SVD_KERNELS[args.precision],
-                         "bound": "tensor", "achieved": achieved, "peak": fp64_peak,
-                         "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if achieved and fp64_peak else None,
-                         "peak_source": "FP64 DGEMM measured in this run (torch.matmul 8192^3, best of 5)",
-                         "achieved_over": "timed region (device time); the SVD phases of concurrent updates overlap",
-                         "svd_stream_ms_sum": mine["svd_ms"], "svd_launches": mine["svd_launches"],
-                         "traffic": None},
+            "roofline": roofline(args, mine, kernel, fp64_peak, hbm_peak),
+            "precision_forms": {form: {
+                "value": r["value"], "unit": "BS-updates/s", "speedup_vs_plain": (r["value"] / plain["value"]) if plain else None,
+                "prob_err_after_timed_layers": (float(np.abs(r["P"] - plain["P"]).max() / abs(plain["trace"]))
+                                                if plain else None),
+                "circuit": r.get("circuit")} for form, r in extras.items()},
             "clocks": mine["clocks"],
             "circuit": circuit,
             "cpu_baseline": cpu,

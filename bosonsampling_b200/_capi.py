@@ -49,6 +49,7 @@ SIGNATURES = {
     "bsmpo_stage_times": (_c_int, [_vp, _dp, _c_int]),
     "bsmpo_set_timing": (_c_int, [_vp, _c_int]),
     "bsmpo_jacobi_timing": (_c_int, [_vp, _dp, _dp, ctypes.POINTER(ctypes.c_int64)]),
+    "bsmpo_tridiag_timing": (_c_int, [_vp, _dp, _dp, _dp, ctypes.POINTER(ctypes.c_int64)]),
     "bsmpo_trace_noalloc": (_c_int, [_c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp]),
 }
 

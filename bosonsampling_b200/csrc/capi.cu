@@ -83,6 +83,11 @@ struct bsmpo_ctx {
   // from and joined to `stream` with events
   cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t fork_ev = nullptr, join_ev[3] = {nullptr, nullptr, nullptr};
+  // tridiagonalisation phase timing (timing mode): events around the forked launches,
+  // read at the update's kept-count synchronisation; streamed bytes and zhetrd flops
+  cudaEvent_t td_ev0 = nullptr, td_ev1 = nullptr;
+  double td_ms = 0.0, td_bytes = 0.0, td_flops = 0.0;
+  int64_t td_phases = 0;
   // BSMPO_GRAM_POLICY (Gram route): 0 (default) exact Jacobi only where the candidates
   // cannot exceed chi; 1 also after a selection that keeps fewer than chi; 2 also where
   // the centre bond holds fewer than chi vectors
@@ -644,6 +649,13 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
         }
       }
       const cudaStream_t ts[4] = {st, h->aux[0], h->aux[1], h->aux[2]};
+      if (h->timing) {
+        if (!h->td_ev0) {
+          CK(h, cudaEventCreate(&h->td_ev0));
+          CK(h, cudaEventCreate(&h->td_ev1));
+        }
+        CK(h, cudaEventRecord(h->td_ev0, st));
+      }
       CK(h, cudaEventRecord(h->fork_ev, st));
       for (int i = 0; i < 3; ++i)
         if (P.td_count[2 - i] > 0) CK(h, cudaStreamWaitEvent(h->aux[i], h->fork_ev, 0));
@@ -654,6 +666,7 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
           CK(h, cudaStreamWaitEvent(st, h->join_ev[i], 0));
         }
       for (int c = 0; c < 4; ++c) h->launches += P.td_count[c] > 0;
+      if (h->timing) CK(h, cudaEventRecord(h->td_ev1, st));
     }
     CK(h, launch_bisect(sd_d, ns, P.max_k, dbuf_d, ebuf_d, lam_d, reinterpret_cast<double*>(h->sig.p),
                         reinterpret_cast<double*>(h->invsig.p), st));
@@ -813,6 +826,16 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
     // reduction of a k x k Hermitian matrix (16/3 k^3, LAPACK's zhetrd count)
     for (const SectorDesc& S : P.sd)
       h->jac_flops += 8.0 * (double)S.k * S.k * S.rows_g + 16.0 / 3.0 * (double)S.k * S.k * S.k;
+    float tms = 0.f;
+    CK(h, cudaEventElapsedTime(&tms, h->td_ev0, h->td_ev1));
+    h->td_ms += tms;
+    h->td_phases++;
+    for (const SectorDesc& S : P.sd) {
+      // step j reads and writes the (k - j - 1)^2 trailing matrix once: 32 B per entry
+      const double k = S.k;
+      h->td_bytes += 32.0 * (k - 1.0) * k * (2.0 * k - 1.0) / 6.0;
+      h->td_flops += 16.0 / 3.0 * k * k * k;
+    }
   }
   if ((rc = clk.mark(4))) return rc;
   // 5. V (Jacobi: extracted from the converged columns; Gram route: eigenvectors, and
@@ -1008,6 +1031,8 @@ void free_workspaces(bsmpo_ctx* h) {
   for (cudaEvent_t& e : h->poll_ev)
     if (e) cudaEventDestroy(e);
   if (h->fork_ev) cudaEventDestroy(h->fork_ev);
+  if (h->td_ev0) cudaEventDestroy(h->td_ev0);
+  if (h->td_ev1) cudaEventDestroy(h->td_ev1);
   for (int i = 0; i < 3; ++i) {
     if (h->aux[i]) { cudaStreamSynchronize(h->aux[i]); cudaStreamDestroy(h->aux[i]); }
     if (h->join_ev[i]) cudaEventDestroy(h->join_ev[i]);
@@ -1156,6 +1181,9 @@ int run_mesh_concurrent(bsmpo_ctx* h, int n_bs, const int* modes, const cplx* u3
     h->jac_ms += w->jac_ms;
     h->jac_flops += w->jac_flops;
     h->jac_launches += w->jac_launches;
+    h->td_ms += w->td_ms; h->td_bytes += w->td_bytes; h->td_flops += w->td_flops; h->td_phases += w->td_phases;
+    w->td_ms = w->td_bytes = w->td_flops = 0.0;
+    w->td_phases = 0;
     for (int q = 0; q < 8; ++q) h->stage_ms[q] += w->stage_ms[q];
     w->launches = w->updates = w->jacobi_rounds = w->jac_launches = 0;
     w->jac_ms = w->jac_flops = 0.0;
@@ -1660,6 +1688,17 @@ int bsmpo_set_timing(bsmpo_ctx* h, int on) {
   h->timing = on != 0;
   h->jac_ms = h->jac_flops = 0.0;
   h->jac_launches = 0;
+  h->td_ms = h->td_bytes = h->td_flops = 0.0;
+  h->td_phases = 0;
+  return BSMPO_OK;
+}
+
+int bsmpo_tridiag_timing(const bsmpo_ctx* h, double* ms, double* bytes, double* flops, int64_t* phases) {
+  if (!h) return fail(nullptr, BSMPO_EINVAL, "null handle");
+  if (ms) *ms = h->td_ms;
+  if (bytes) *bytes = h->td_bytes;
+  if (flops) *flops = h->td_flops;
+  if (phases) *phases = h->td_phases;
   return BSMPO_OK;
 }
 

@@ -252,6 +252,15 @@ class MPOSimulator:
         self._chk(self.L.bsmpo_jacobi_timing(self.h, _capi.dptr(ms), _capi.dptr(fl), ctypes.byref(n)))
         return float(ms[0]), float(fl[0]), int(n.value)
 
+    def tridiag_timing(self):
+        """(device ms, streamed bytes, zhetrd flops, phases) of the Gram route's
+        tridiagonalisation since set_timing()."""
+        ms, by, fl = np.zeros(1), np.zeros(1), np.zeros(1)
+        n = ctypes.c_int64()
+        self._chk(self.L.bsmpo_tridiag_timing(self.h, _capi.dptr(ms), _capi.dptr(by), _capi.dptr(fl),
+                                              ctypes.byref(n)))
+        return float(ms[0]), float(by[0]), float(fl[0]), int(n.value)
+
     def stage_times(self):
         """Per-stage milliseconds (only with BSMPO_PROFILE=1 at creation)."""
         ms = np.zeros(10)

@@ -226,6 +226,13 @@ int bsmpo_set_timing(bsmpo_ctx* h, int on);
  * reduction) per sector; 8 flops per complex MAC. */
 int bsmpo_jacobi_timing(const bsmpo_ctx* h, double* ms, double* flops, int64_t* launches);
 
+/* Device time (ms) of the Householder tridiagonalisation phase of the Gram route (its
+ * forked size-class launches, CUDA events on the update's stream) since
+ * bsmpo_set_timing(h, 1), with the bytes its fused passes stream (every step reads and
+ * writes the trailing matrix once: 32 B per complex entry) and its flops (16/3 k^3 per
+ * sector, LAPACK's zhetrd count), and the number of phases. */
+int bsmpo_tridiag_timing(const bsmpo_ctx* h, double* ms, double* bytes, double* flops, int64_t* phases);
+
 /* Stage timing, filled only when the handle was created with BSMPO_PROFILE=1 in the
  * environment (each stage then ends with a stream synchronisation).  ms[0..7]:
  * plan+upload, Theta GEMM, mix, Jacobi rounds, finish+select+sync, V/W, scatter,
