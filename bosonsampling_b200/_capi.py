@@ -23,6 +23,8 @@ SIGNATURES = {
     "bsmpo_unitary_tr": (_c_int, [_c_int, _c_double, _c_double, _c_double, _c_double, _vp, _vp, _vp]),
     "bsmpo_contract_sector": (_c_int, [_c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp,
                                        _c_int, _c_int, _c_int, _vp, _vp]),
+    "bsmpo_contract_mps": (_c_int, [_c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                    _c_int, _c_int, _c_int, _vp, _vp]),
     "bsmpo_zgemm_tf32x3": (_c_int, [_c_int, _c_int, _c_int, _vp, _c_int, _c_int, _vp, _c_int, _vp, _c_int,
                                     _vp]),
     "bsmpo_create": (_c_int, [_c_int, _c_int, _c_int, _c_int, ctypes.POINTER(_vp)]),

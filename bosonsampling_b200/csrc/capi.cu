@@ -1273,6 +1273,20 @@ int bsmpo_contract_sector(int d, int cc0, int cc1, const void* u, const void* gl
   return BSMPO_OK;
 }
 
+int bsmpo_contract_mps(int d, int tau, const void* u, const void* glc, const void* gcr, const double* ll,
+                       const double* lc, const double* lr, const int* cl, const int* cc, const int* cr,
+                       int len_l, int len_c, int len_r, void* t, void* stream) {
+  if (d < 1 || d > BSMPO_MAX_D || len_l < 0 || len_c < 0 || len_r < 0 || !u || !t)
+    return fail(nullptr, BSMPO_EINVAL, "bad argument");
+  if (tau < 0 || tau >= d) return fail(nullptr, BSMPO_EINVAL, "bad centre charge");
+  if ((len_l > 0 && (!glc || !ll || !cl)) || (len_r > 0 && (!gcr || !lr || !cr)) || (len_c > 0 && (!lc || !cc)))
+    return fail(nullptr, BSMPO_EINVAL, "null input");
+  cudaError_t e = launch_contract_mps(d, tau, u, glc, gcr, ll, lc, lr, cl, cc, cr, len_l, len_c, len_r, t,
+                                      (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(nullptr, BSMPO_ECUDA, cudaGetErrorString(e));
+  return BSMPO_OK;
+}
+
 int bsmpo_zgemm_tf32x3(int M, int N, int K, const void* a, int lda, int opA, const void* b, int ldb,
                        void* c, int ldc, void* stream) {
   if (M < 0 || N < 0 || K < 1 || !a || !b || !c || (opA != 0 && opA != 1) || ldb < N || ldc < N ||

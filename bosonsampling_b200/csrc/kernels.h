@@ -220,6 +220,12 @@ cudaError_t launch_contract_sector(int d, int cc0, int cc1, const void* u, const
 cudaError_t launch_product_fill(int n, int d, int chi, const int* charge, const void* rho,
                                 void* gamma, cudaStream_t s);
 
+// Pure-state (MPS) variant of the contraction, one int32 charge per index.
+cudaError_t launch_contract_mps(int d, int tau, const void* u, const void* glc, const void* gcr,
+                                const double* ll, const double* lc, const double* lr, const int* cl,
+                                const int* cc, const int* cr, int len_l, int len_c, int len_r, void* t,
+                                cudaStream_t s);
+
 // ---------------------------------------------------------------- observables.cu
 // env_r[b] (b = n..0) and env_l[b] (b = 0..n), complex, masked to ket == bra charges.
 cudaError_t launch_env_right_step(int d, int chi, const void* gamma_b, const int* charge_b,

@@ -88,3 +88,39 @@ def update_MPO(d, charge_c_0, charge_c_1, U_r, U_i, glc_obj, gcr_obj, cl_obj, cr
         ctypes.c_void_p(cr.data_ptr()), int(len_l), int(len_c), int(len_r),
         ctypes.c_void_p(C.data_ptr()), stream))
     return C
+
+
+def update_MPS(d, tau, U_r, U_i, Glc, Gcr, LL, LC, LR, CL, CC, CR, incC):
+    """The pure-state (MPS) two-site contraction, as ``update_MPS``
+    (``src/cuda_kernels.py:72-90``, kernel ``src/update_kernel.cu:193-769``):
+    ``T[l, r] = LL[l] LR[r] sum_c LC[c] Glc[l, c] Gcr[c, r] U[cl - tau, tau - cr, cl - q(c)]``
+    over centre entries with ``cl >= q(c) >= cr``.  ``CC`` holds the centre charge of
+    every centre index (``incC``, the reference's first-index-per-charge table, is
+    accepted for the signature and checked against it).  Returns T [len_l, len_r]
+    complex128 (FP64 throughout; the reference computes in FP32)."""
+    torch = _torch()
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    def cdev(x, dtype):
+        return torch.as_tensor(_data(x), device=dev).to(dtype).contiguous()
+
+    glc, gcr = cdev(Glc, torch.complex128), cdev(Gcr, torch.complex128)
+    ll, lc, lr = cdev(LL, torch.float64), cdev(LC, torch.float64), cdev(LR, torch.float64)
+    cl, cc, cr = cdev(CL, torch.int32), cdev(CC, torch.int32), cdev(CR, torch.int32)
+    len_l, len_c = glc.shape
+    len_r = gcr.shape[1]
+    inc = np.asarray(torch.as_tensor(incC).cpu()).reshape(-1)
+    ccn = cc.cpu().numpy()
+    for q, first in enumerate(inc):
+        if first >= 0 and first < len_c and ccn[first] != q:
+            raise ValueError("incC[%d] = %d does not match the centre charges" % (q, first))
+    U = (torch.as_tensor(U_r, device=dev).to(torch.float64)
+         + 1j * torch.as_tensor(U_i, device=dev).to(torch.float64)).to(torch.complex128).contiguous()
+    T = torch.empty((len_l, len_r), dtype=torch.complex128, device=dev)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    vp = ctypes.c_void_p
+    _capi.check(_capi.lib().bsmpo_contract_mps(
+        int(d), int(tau), vp(U.data_ptr()), vp(glc.data_ptr()), vp(gcr.data_ptr()), vp(ll.data_ptr()),
+        vp(lc.data_ptr()), vp(lr.data_ptr()), vp(cl.data_ptr()), vp(cc.data_ptr()), vp(cr.data_ptr()),
+        int(len_l), int(len_c), int(len_r), vp(T.data_ptr()), stream))
+    return T

@@ -74,6 +74,19 @@ int bsmpo_contract_sector(int d, int cc0, int cc1, const void* u,
                           const int* cl, const int* cc, const int* cr,
                           int len_l, int len_c, int len_r, void* c, void* stream);
 
+/* The pure-state (MPS) variant of the contraction.  Replaces cuda_kernels.update_MPS /
+ * update_kernel.cu:kernel (src/cuda_kernels.py:72-90, src/update_kernel.cu:193-769),
+ * one charge (photon number) per bond index:
+ *   T[l][r] = LL[l] LR[r] sum_c LC[c] Glc[l][c] Gcr[c][r] U(cl - tau, tau - cr, cl - q(c))
+ * over c with cl >= q(c) >= cr (else the term is 0; T is 0 where cl - tau or tau - cr
+ * falls outside [0, d)).
+ *   u    device complex128 [d][d][d]; glc [len_l][len_c]; gcr [len_c][len_r]
+ *   ll, lc, lr device double Lambda of the rows / centre entries / columns
+ *   cl, cc, cr device int32 charges; t device complex128 [len_l][len_r] (overwritten). */
+int bsmpo_contract_mps(int d, int tau, const void* u, const void* glc, const void* gcr, const double* ll,
+                       const double* lc, const double* lr, const int* cl, const int* cc, const int* cr,
+                       int len_l, int len_c, int len_r, void* t, void* stream);
+
 /* Complex GEMM on the tensor cores with three TF32 split products (hi*hi + hi*lo +
  * lo*hi, FP32 accumulation): C[m][n] = sum_k op(A)[m][k] B[k][n], the contraction
  * primitive of BSMPO_PRECISION_TF32X3 (the reference's update_MPO_kernel.cu GEMM,

@@ -128,6 +128,38 @@ def test_update_mpo_dropin_matches_oracle_block_product():
             np.testing.assert_allclose(C, ref, atol=1e-13 * scale)
 
 
+@pytest.mark.parametrize("d,tau", [(3, 1), (4, 2), (5, 0), (5, 4)])
+def test_update_mps_dropin_matches_elementwise_sum(d, tau):
+    """The MPS variant (src/update_kernel.cu:193-769) against an element-wise
+    restatement of its sum: T[l, r] = LL LR sum_c LC Glc Gcr U[cl - tau, tau - cr, cl - q]."""
+    from bosonsampling_b200 import cuda_kernels
+    rng = np.random.default_rng(10 * d + tau)
+    len_l, len_c, len_r = 37, 29, 41
+    CL = np.sort(rng.integers(0, d, len_l))[::-1].astype(np.int32)
+    CC = np.sort(rng.integers(0, d, len_c)).astype(np.int32)
+    CR = np.sort(rng.integers(0, d, len_r))[::-1].astype(np.int32)
+    inc = np.full(d, -1, np.int32)
+    for i, q in enumerate(CC):
+        if inc[q] < 0:
+            inc[q] = i
+    Glc = rng.standard_normal((len_l, len_c)) + 1j * rng.standard_normal((len_l, len_c))
+    Gcr = rng.standard_normal((len_c, len_r)) + 1j * rng.standard_normal((len_c, len_r))
+    LL, LC, LR = (rng.uniform(0.1, 1.0, n) for n in (len_l, len_c, len_r))
+    U3 = fock.update_tensor(interferometer.t_block(0.7, 0.3), d)
+    Ut = torch.from_numpy(U3.real.copy()).cuda(), torch.from_numpy(U3.imag.copy()).cuda()
+    T = cuda_kernels.update_MPS(d, tau, Ut[0], Ut[1], Glc, Gcr, LL, LC, LR, CL, CC, CR, inc).cpu().numpy()
+    ref = np.zeros((len_l, len_r), dtype=np.complex128)
+    for i, a in enumerate(CL):
+        for j, b in enumerate(CR):
+            if not (0 <= a - tau < d and 0 <= tau - b < d):
+                continue
+            for c, q in enumerate(CC):
+                if a >= q >= b and a - q < d:
+                    ref[i, j] += LC[c] * U3[a - tau, tau - b, a - q] * Glc[i, c] * Gcr[c, j]
+            ref[i, j] *= LL[i] * LR[j]
+    np.testing.assert_allclose(T, ref, atol=1e-13 * max(np.abs(ref).max(), 1e-300))
+
+
 # ------------------------------------------------------------------ one BS update
 @pytest.mark.parametrize("case", [(8, 3, 32, 5), (10, 4, 48, 12), (12, 5, 64, 20)])
 def test_single_update_sigma_kept_and_weight(case):
