@@ -68,6 +68,10 @@ def parse():
     p.add_argument("--also", default="tf32x3",
                    help="comma-separated further precision forms timed on the same layers and "
                         "checked over the whole circuit ('' for none)")
+    p.add_argument("--batch", type=int, default=16,
+                   help="independent circuits of the batched workload (N in [16, 48], eta in "
+                        "[0.2, 0.8], d=4, chi in {128, 256, 512}) run side by side and one by one "
+                        "(0: skip)")
     p.add_argument("--no-plain", action="store_true",
                    help="skip the plain FP64 path (the metric's denominator) and the error against it")
     p.add_argument("--bs-slice", default=None,
@@ -560,6 +564,31 @@ def main():
                                            "value": replica_rate(len(bs), world, t_f),
                                            "prob_err_vs_fp64": float(np.abs(P_f - P_p).max() / abs(trace_p))}
 
+    # ---- batched form: independent circuits of uneven N and chi, side by side against one
+    # by one (host wall clock; every circuit is computed exactly as alone)
+    batched = None
+    if args.batch > 0 and not args.bs_slice and world == 1:
+        specs = engine.batch_circuits(n_circuits=args.batch)
+        n_up = sum(len(sp["mesh"]) for sp in specs)
+        engine.run_batch(specs[:2], concurrency=2, precision=args.precision)   # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        engine.run_batch(specs, concurrency=1, precision=args.precision, workers=8)
+        torch.cuda.synchronize()
+        t_seq = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        engine.run_batch(specs, concurrency=8, precision=args.precision, workers=4)
+        torch.cuda.synchronize()
+        t_par = time.perf_counter() - t0
+        batched = {"circuits": len(specs), "bs_updates": n_up,
+                   "value": n_up / t_par, "one_by_one_value": n_up / t_seq, "unit": "BS-updates/s",
+                   "speedup": t_seq / t_par, "seconds": round(t_par, 3), "one_by_one_seconds": round(t_seq, 3),
+                   "n_range": [min(sp["n"] for sp in specs), max(sp["n"] for sp in specs)],
+                   "chis": sorted(set(sp["chi"] for sp in specs)),
+                   "how": "8 circuits at a time, one handle + host thread + stream each, 4 worker streams per "
+                          "handle; one by one: 8 worker streams; host wall clock, whole circuits with "
+                          "initial state, phases and observables"}
+
     # ---- roofline of the dominant phase: the SVD step (Jacobi rounds, or the Gram GEMM,
     # Householder reduction and bisection of the Gram route), FP64 against measured DGEMM
     fp64_peak = measure_fp64_peak(torch) if rank == 0 else None
@@ -608,6 +637,7 @@ def main():
                 "circuit": r.get("circuit")} for form, r in extras.items()},
             "clocks": mine["clocks"],
             "circuit": circuit,
+            "batched": batched,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))

@@ -270,3 +270,57 @@ class MPOSimulator:
         out["jacobi_rounds"] = int(ms[8])
         out["updates"] = int(ms[9])
         return out
+
+
+def batch_circuits(n_circuits=64, seed=1004, chis=(128, 256, 512), d=4):
+    """Independent seeded circuits of uneven size: N uniform in [16, 48], single photons in
+    every second mode, transmissivity uniform in [0.2, 0.8], chi drawn from ``chis``; the
+    Haar unitary of circuit i is seeded by ``seed * 1000 + i``."""
+    from . import interferometer
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_circuits):
+        n = int(rng.integers(16, 49))
+        eta = float(rng.uniform(0.2, 0.8))
+        chi = int(rng.choice(np.asarray(chis)))
+        U, bs, ph = interferometer.circuit(n, seed * 1000 + i)
+        specs.append(dict(n=n, d=d, chi=chi, eta=eta, photon_modes=list(range(0, n, 2)), mesh=bs, phases=ph))
+    return specs
+
+
+def run_batch(specs, concurrency=8, precision="fp64-gram", workers=4):
+    """Runs independent circuits (``batch_circuits`` entries) side by side on the current
+    device: ``concurrency`` circuits at a time, each on its own handle, host thread and
+    stream (the library's calls release the GIL), each handle overlapping its own
+    updates on ``workers`` streams.  Returns ``[(trace, marginals)]`` in input order;
+    every circuit computes exactly what it computes alone."""
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+    dev = torch.cuda.current_device()
+    out = [None] * len(specs)
+    lock = threading.Lock()
+
+    def one(i):
+        sp = specs[i]
+        torch.cuda.set_device(dev)
+        with torch.cuda.stream(torch.cuda.Stream()):
+            with MPOSimulator(sp["n"], sp["d"], sp["chi"]) as sim:
+                sim.set_precision(precision)
+                sim.set_workers(workers)
+                sim.init_single_photons(sp["photon_modes"], sp["eta"])
+                m = sp["mesh"]
+                sim.run_mesh([b[1] for b in m], [b[2] for b in m], [b[3] for b in m])
+                sim.apply_phases(sp["phases"])
+                res = sim.observables()
+        with lock:
+            out[i] = res
+
+    if concurrency <= 1:
+        for i in range(len(specs)):
+            one(i)
+    else:
+        with ThreadPoolExecutor(max_workers=concurrency) as ex:
+            list(ex.map(one, range(len(specs))))
+    return out
