@@ -46,7 +46,10 @@ def Rand_U(d: int, r: float):
 
 
 def _data(x):
-    return x.data if hasattr(x, "data") and not hasattr(x, "data_ptr") else x
+    """The array inside the reference's ``Data`` wrapper (``src/mpo_sort.py:6-36``), or x."""
+    if isinstance(x, np.ndarray) or hasattr(x, "data_ptr"):
+        return x
+    return x.data if hasattr(x, "data") else x
 
 
 def update_MPO(d, charge_c_0, charge_c_1, U_r, U_i, glc_obj, gcr_obj, cl_obj, cr_obj,
