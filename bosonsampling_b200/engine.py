@@ -288,39 +288,53 @@ def batch_circuits(n_circuits=64, seed=1004, chis=(128, 256, 512), d=4):
     return specs
 
 
-def run_batch(specs, concurrency=8, precision="fp64-gram", workers=4):
+def run_batch(specs, concurrency=8, precision="fp64-gram", workers=4, timing=None):
     """Runs independent circuits (``batch_circuits`` entries) side by side on the current
     device: ``concurrency`` circuits at a time, each on its own handle, host thread and
-    stream (the library's calls release the GIL), each handle overlapping its own
-    updates on ``workers`` streams.  Returns ``[(trace, marginals)]`` in input order;
-    every circuit computes exactly what it computes alone."""
-    import threading
+    stream (the library's calls release the GIL), each handle overlapping its own updates
+    on ``workers`` streams.  Handles are created and initialised first and released last,
+    outside the concurrent phase (allocating or freeing device memory synchronises the
+    whole device).  Returns ``[(trace, marginals)]`` in input order; every circuit
+    computes exactly what it computes alone.  ``timing`` (a dict), if given, receives the
+    wall-clock seconds of the concurrent phase (the meshes, phases and observables)."""
+    import time
     from concurrent.futures import ThreadPoolExecutor
 
     import torch
     dev = torch.cuda.current_device()
-    out = [None] * len(specs)
-    lock = threading.Lock()
-
-    def one(i):
-        sp = specs[i]
-        torch.cuda.set_device(dev)
-        with torch.cuda.stream(torch.cuda.Stream()):
-            with MPOSimulator(sp["n"], sp["d"], sp["chi"]) as sim:
+    streams = [torch.cuda.Stream() for _ in specs]
+    sims = []
+    try:
+        for sp, st in zip(specs, streams):
+            with torch.cuda.stream(st):
+                sim = MPOSimulator(sp["n"], sp["d"], sp["chi"])
+                sims.append(sim)
                 sim.set_precision(precision)
                 sim.set_workers(workers)
                 sim.init_single_photons(sp["photon_modes"], sp["eta"])
+        torch.cuda.synchronize()
+        out = [None] * len(specs)
+
+        def one(i):
+            sp, sim = specs[i], sims[i]
+            torch.cuda.set_device(dev)
+            with torch.cuda.stream(streams[i]):
                 m = sp["mesh"]
                 sim.run_mesh([b[1] for b in m], [b[2] for b in m], [b[3] for b in m])
                 sim.apply_phases(sp["phases"])
-                res = sim.observables()
-        with lock:
-            out[i] = res
+                out[i] = sim.observables()
 
-    if concurrency <= 1:
-        for i in range(len(specs)):
-            one(i)
-    else:
-        with ThreadPoolExecutor(max_workers=concurrency) as ex:
-            list(ex.map(one, range(len(specs))))
-    return out
+        t0 = time.perf_counter()
+        if concurrency <= 1:
+            for i in range(len(specs)):
+                one(i)
+        else:
+            with ThreadPoolExecutor(max_workers=concurrency) as ex:
+                list(ex.map(one, range(len(specs))))
+        torch.cuda.synchronize()
+        if timing is not None:
+            timing["seconds"] = time.perf_counter() - t0
+        return out
+    finally:
+        for sim in sims:
+            sim.close()
