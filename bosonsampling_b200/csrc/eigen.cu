@@ -22,6 +22,8 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -578,7 +580,20 @@ int eigen_max_k() {
   return std::min(k, 32 * 32);   // the back-transformation keeps 32 entries per lane
 }
 
-int tridiag_class(int k) { return k <= 64 ? 0 : k <= 160 ? 1 : k <= 320 ? 2 : 3; }
+// Size-class bounds (largest k of classes 0, 1, 2); BSMPO_TD_CLASSES="a,b,c" in the
+// environment replaces them (read once).
+int tridiag_class(int k) {
+  static const int* bounds = [] {
+    static int b[3] = {64, 160, 320};
+    const char* e = std::getenv("BSMPO_TD_CLASSES");
+    int x, y, z;
+    if (e && std::sscanf(e, "%d,%d,%d", &x, &y, &z) == 3 && 0 < x && x < y && y < z) {
+      b[0] = x; b[1] = y; b[2] = z;
+    }
+    return b;
+  }();
+  return k <= bounds[0] ? 0 : k <= bounds[1] ? 1 : k <= bounds[2] ? 2 : 3;
+}
 
 cudaError_t launch_tridiag(const SectorDesc* sd_dev, const int* list_dev, const int* class_count,
                            const int* class_kmax, void* gbuf, double* dbuf, double* ebuf,
