@@ -77,6 +77,7 @@ struct bsmpo_ctx {
   // tensor-core contractions (BSMPO_PRECISION_TF32X3): groups and tensor maps of the
   // V / W GEMMs, and the pipeline's error word
   DevBuf tab3, tcerr;
+  DevBuf jwork;   // executed Jacobi rows: pair-Gram rows, rotated rows (unsigned long long[2])
   HostStage stage3;
   int precision = BSMPO_PRECISION_FP64;
   // the tridiagonalisation's size classes run side by side: three more streams, forked
@@ -680,6 +681,8 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
     CKL(h, launch_sector_norms(sd_d, ns, h->abuf.p, nf2, st));
     CK(h, cudaMemsetAsync(h->rot.p, 0, (size_t)3 * ns * sizeof(int), st));
     CK(h, cudaMemsetAsync(h->pcnt.p, 0, std::max(P.jac_slots, 1) * sizeof(int), st));
+    if ((rc = grow(h, h->jwork, 2 * sizeof(unsigned long long)))) return rc;
+    CK(h, cudaMemsetAsync(h->jwork.p, 0, 2 * sizeof(unsigned long long), st));
     // Convergence polls run one chunk behind: after launching chunk c + 1 the host reads
     // the counters copied after chunk c, so the stream always has a chunk queued while the
     // host checks (a converged sector's rounds in the extra chunk exit at once).  Counters
@@ -705,7 +708,8 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
         CK(h, launch_jacobi_round(sd_d, jw_d, (int)active.size(), gram_ctas, apply_ctas, t,
                                   h->abuf.p, reinterpret_cast<int*>(h->rot.p), nf2, 0.0, MAX_SWEEPS,
                                   h->pbuf.p, reinterpret_cast<int*>(h->pcnt.p), h->qbuf.p,
-                                  reinterpret_cast<int*>(h->qflag.p), st));
+                                  reinterpret_cast<int*>(h->qflag.p),
+                                  reinterpret_cast<unsigned long long*>(h->jwork.p), st));
         h->launches += 2;
       }
       CK(h, cudaMemcpyAsync(hrot_slot[slot], h->rot.p, (size_t)3 * ns * sizeof(int),
@@ -748,7 +752,11 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
       }
       cur ^= 1;
     }
-    if (h->timing) CK(h, cudaEventRecord(h->ev1, st));
+    if (h->timing) {
+      CK(h, cudaMemcpyAsync(static_cast<char*>(h->hres.p) + 2048, h->jwork.p, 2 * sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, st));
+      CK(h, cudaEventRecord(h->ev1, st));
+    }
     // sweeps the slowest sector needed (its last one without rotations included); t also
     // counts the chunk queued after convergence, whose rounds exit at once
     {
@@ -763,15 +771,13 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
       CK(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
       h->jac_ms += ms;
       h->jac_launches += t;
-      // algorithmic flops of the executed sweeps: per block pair and round the pair
-      // Gram (rows_g) and the rotation (rows_tot) of 32 columns, 8 flops per complex MAC
-      for (int s = 0; s < ns; ++s) {
-        const SectorDesc& S = P.sd[s];
-        const double sweeps = conv_at[s] > 0 ? conv_at[s] : (double)t / P.jw[s].rounds;
-        const double cols = 2.0 * jacobi_block_cols();
-        h->jac_flops += sweeps * P.jw[s].rounds * P.jw[s].npairs * 8.0 * cols * cols *
-                        ((double)S.rows_g + S.rows_tot);
-      }
+      // flops of the executed work, counted on the device: every row that formed a
+      // partial pair Gram contributes its 10 upper 8 x 8 tiles (640 complex MACs), every
+      // rotated row 32 x 32 complex MACs; 8 flops per complex MAC.  Pairs that did not
+      // rotate and sectors that had converged do no apply work and are not counted.
+      const unsigned long long* hw =
+          reinterpret_cast<const unsigned long long*>(static_cast<char*>(h->hres.p) + 2048);
+      h->jac_flops += 8.0 * 640.0 * (double)hw[0] + 8.0 * 1024.0 * (double)hw[1];
     }
     if ((rc = clk.mark(3))) return rc;
     if (!converged) {
@@ -1018,7 +1024,7 @@ void free_workspaces(bsmpo_ctx* h) {
                     &h->perm, &h->tab, &h->tab2, &h->rot, &h->kept, &h->u3, &h->m4,
                     &h->env_l, &h->env_r, &h->part, &h->outv, &h->dims, &h->nf2, &h->qbuf,
                     &h->qflag, &h->pbuf, &h->pcnt, &h->gbuf, &h->eigd, &h->taub, &h->invsig,
-                    &h->escr, &h->swp, &h->zbuf, &h->ybuf, &h->tab3, &h->tcerr};
+                    &h->escr, &h->swp, &h->zbuf, &h->ybuf, &h->tab3, &h->tcerr, &h->jwork};
   for (DevBuf* b : bufs)
     if (b->p) cudaFreeAsync(b->p, h->stream);
   cudaStreamSynchronize(h->stream);

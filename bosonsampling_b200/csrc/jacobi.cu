@@ -140,7 +140,8 @@ __global__ __launch_bounds__(JNT) void jacobi_gram_kernel(const SectorDesc* __re
                                                           cplx* __restrict__ pbuf,
                                                           int* __restrict__ pcnt,
                                                           cplx* __restrict__ qbuf,
-                                                          int* __restrict__ qflag) {
+                                                          int* __restrict__ qflag,
+                                                          unsigned long long* __restrict__ executed) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   GramSmem& S = *reinterpret_cast<GramSmem*>(smem_raw);
   const int tid = threadIdx.x;
@@ -219,6 +220,7 @@ __global__ __launch_bounds__(JNT) void jacobi_gram_kernel(const SectorDesc* __re
     }
   }
   __syncthreads();   // the tile is dead; G takes its place
+  if (tid == 0) atomicAdd(executed, (unsigned long long)ng);   // executed: ng rows of 10 Gram tiles
   const int cs_g = T.W.cs_g;
   if (cs_g == 1) {
 #pragma unroll
@@ -410,7 +412,8 @@ __global__ __launch_bounds__(JNT) void jacobi_apply_kernel(const SectorDesc* __r
                                                            int n_work, int t, cplx* __restrict__ abuf,
                                                            int max_sweeps,
                                                            const cplx* __restrict__ qbuf,
-                                                           const int* __restrict__ qflag) {
+                                                           const int* __restrict__ qflag,
+                                                           unsigned long long* __restrict__ executed) {
   __shared__ double2 Qs[JC][JC + 1];
   __shared__ double Qsum[JC][JC + 1];   // Re Q + Im Q
   __shared__ int cols[JC];
@@ -422,6 +425,7 @@ __global__ __launch_bounds__(JNT) void jacobi_apply_kernel(const SectorDesc* __r
   const int k = D.k;
   const int r0 = T.part * T.W.chunk;
   const int nr = min(D.rows_tot, r0 + T.W.chunk) - r0;
+  if (tid == 0) atomicAdd(executed + 1, (unsigned long long)nr);   // executed: nr rows rotated
   if (tid < JC) cols[tid] = jac_col(T, tid, k);
   const cplx* qi = qbuf + (int64_t)T.slot * JC * JC;
 #pragma unroll
@@ -567,7 +571,8 @@ cudaError_t launch_sector_norms(const SectorDesc* sd_dev, int n_sectors, const v
 cudaError_t launch_jacobi_round(const SectorDesc* sd_dev, const JacobiWork* work_dev, int n_work,
                                 int gram_ctas, int apply_ctas, int t, void* abuf, int* rot_count,
                                 const double* nf2, double tol, int max_sweeps, void* pbuf,
-                                int* pcnt, void* qbuf, int* qflag, cudaStream_t s) {
+                                int* pcnt, void* qbuf, int* qflag, unsigned long long* executed,
+                                cudaStream_t s) {
   if (gram_ctas <= 0) return cudaSuccess;
   const int smem1 = (int)sizeof(GramSmem);
   // once per process (thread-safe initialisation; several host threads launch rounds)
@@ -576,12 +581,12 @@ cudaError_t launch_jacobi_round(const SectorDesc* sd_dev, const JacobiWork* work
   if (attr != cudaSuccess) return attr;
   jacobi_gram_kernel<<<gram_ctas, JNT, smem1, s>>>(
       sd_dev, work_dev, n_work, t, reinterpret_cast<const cplx*>(abuf), rot_count, nf2, tol,
-      max_sweeps, reinterpret_cast<cplx*>(pbuf), pcnt, reinterpret_cast<cplx*>(qbuf), qflag);
+      max_sweeps, reinterpret_cast<cplx*>(pbuf), pcnt, reinterpret_cast<cplx*>(qbuf), qflag, executed);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   jacobi_apply_kernel<<<apply_ctas, JNT, 0, s>>>(sd_dev, work_dev, n_work, t,
                                                  reinterpret_cast<cplx*>(abuf), max_sweeps,
-                                                 reinterpret_cast<const cplx*>(qbuf), qflag);
+                                                 reinterpret_cast<const cplx*>(qbuf), qflag, executed);
   return cudaGetLastError();
 }
 

@@ -143,11 +143,13 @@ int jacobi_block_cols();
 // One round of every listed sector: the gram kernel (partial Grams -> pbuf, 32 x 32
 // complex per gram CTA; the last part of a pair reduces, tests and solves, writing Q
 // and the flag of its slot), then the apply kernel.  pcnt (one int per slot) must be
-// zero before the first round; the kernels leave it zero.
+// zero before the first round; the kernels leave it zero.  executed[0] / executed[1]
+// count the rows that formed a partial pair Gram / were rotated (the executed work).
 cudaError_t launch_jacobi_round(const SectorDesc* sd_dev, const JacobiWork* work_dev, int n_work,
                                 int gram_ctas, int apply_ctas, int t, void* abuf, int* rot_count,
                                 const double* nf2, double tol, int max_sweeps, void* pbuf,
-                                int* pcnt, void* qbuf, int* qflag, cudaStream_t s);
+                                int* pcnt, void* qbuf, int* qflag, unsigned long long* executed,
+                                cudaStream_t s);
 // Largest number of Jacobi-matrix rows (|L| + |R| or |L|) a sector may have.
 // ||T_s||_F^2 of each sector's Jacobi matrix (Gram rows), fixed-order reduction.
 cudaError_t launch_sector_norms(const SectorDesc* sd_dev, int n_sectors, const void* abuf,

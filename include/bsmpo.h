@@ -234,9 +234,10 @@ int64_t bsmpo_kernel_launches(const bsmpo_ctx* h);
 int bsmpo_set_timing(bsmpo_ctx* h, int on);
 
 /* Accumulated SVD-phase device time (ms), its algorithmic flops and its launches since
- * bsmpo_set_timing(h, 1).  Jacobi: executed sweeps, pair Gram + rotation of each
- * 32-column block pair; Gram route: 8 k^2 rows (the Gram) + 16/3 k^3 (Householder
- * reduction) per sector; 8 flops per complex MAC. */
+ * bsmpo_set_timing(h, 1).  Jacobi: the executed work counted on the device (rows that
+ * formed a partial pair Gram, 640 complex MACs each, and rotated rows, 1024 each);
+ * Gram route: 8 k^2 rows (the Gram) + 16/3 k^3 (Householder reduction) per sector;
+ * 8 flops per complex MAC. */
 int bsmpo_jacobi_timing(const bsmpo_ctx* h, double* ms, double* flops, int64_t* launches);
 
 /* Device time (ms) of the Householder tridiagonalisation phase of the Gram route (its
