@@ -10,7 +10,8 @@
 //      Q = H_0 ... H_{k-2}, H_j = I - tau_j v_j v_j^H (LAPACK's zhetd2 conventions,
 //      lower storage), one thread-block cluster per sector, rows owned cyclically by
 //      the cluster's CTAs, the rank-2 update of step j - 1 fused with the matrix-vector
-//      product of step j (one read and one write of the trailing matrix per step);
+//      product of step j (one read and one write of the trailing matrix per step), one
+//      cluster barrier per step;
 //   2. every eigenvalue by multisection of Sturm counts (one warp per eigenvalue, 32
 //      points per pass), sigma = sqrt(lambda), zero below the numerical floor;
 //   3. after the global top-chi selection: eigenvectors of the kept eigenvalues by
@@ -77,20 +78,24 @@ __device__ __forceinline__ cplx cdiv(cplx a, cplx b) {
 // ---------------------------------------------------------------------------------
 // 1. Tridiagonalisation.  Cluster c handles sector list[c]; its cl CTAs (1, 2, 4 or 8,
 //    by sector size: a small sector would spend its steps waiting at barriers of a big
-//    cluster) own the rows i = rank (mod cl).  Per step j (trailing size t = k - j - 1):
-//    S0  owner of row j: apply the pending update of step j - 1 to row j, form the
-//        reflector from x = conj(A[j][j+1:]) (zlarfg: beta real), store v_j in row j,
-//        d_j, e_j = beta, tau_j; publish v_j and tau_j in its shared memory;
+//    cluster) own the rows i = rank (mod cl).  Every CTA holds the reflector vectors
+//    and a copy of the row being reduced, so one cluster barrier per step suffices.
+//    Step j (trailing size t = k - j - 1):
+//    R   every CTA (warp 0): row j as the previous pass left it, minus the pending
+//        rank-2 update of step j - 1, gives d_j and the reflector (zlarfg: beta real,
+//        tau_j, v_j), computed redundantly and bit-identically in every CTA (the same
+//        inputs, the same warp reduction);
+//    P   every CTA, its rows i > j: A[i][l] -= v'_i conj(w'_l) + w'_i conj(v'_l) (v', w'
+//        of step j - 1), write back, p_i = tau sum_l A[i][l] v_l, partial
+//        c = sum conj(p_i) v_i; the owner of row j + 1 also publishes that row;
 //    --  cluster barrier
-//    S1  every CTA: copy v_j; for its rows i > j: A[i][l] -= v'_i conj(w'_l) +
-//        w'_i conj(v'_l) (v', w' of step j - 1), write back, p_i = tau sum_l A[i][l] v_l;
-//        partial c = sum conj(p_i) v_i;
-//    --  cluster barrier
-//    S2  c = sum of the partials; every CTA forms the whole w_j = p - tau c / 2 v from
-//        the owners' p (it is v', w' of the next step).
-//    Two cluster barriers per step; S0 is one warp's work.
-// Every row is read and written by its owner only, so the trailing matrix needs no
-// ordering across CTAs; the vectors travel through distributed shared memory.
+//    G   every CTA: c = sum of the partials (fixed order), w_j = p - tau c / 2 v from the
+//        owners' p, and a copy of the published row j + 1 (the next step's R); the owner
+//        of row j stores v_j there for the back-transformation, d_j, e_j = beta, tau_j.
+//    p and the partials are double-buffered by step parity; the published row is written
+//    again only cl steps later: every next write follows the next barrier, which no CTA
+//    passes before every CTA has finished its G.
+// Every row of the trailing matrix is read and written by its owner only.
 __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
     tridiag_kernel(const SectorDesc* __restrict__ sd, const int* __restrict__ list, int kmax,
                    cplx* __restrict__ gbuf, double* __restrict__ dbuf, double* __restrict__ ebuf,
@@ -101,13 +106,13 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
   const int TD_CL = (int)cluster.num_blocks();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int own_cap = kmax / TD_CL + 1;
-  // v and w of two consecutive steps (ping-pong): vb + (j & 1) kmax, wb + (j & 1) kmax
-  cplx* vb = reinterpret_cast<cplx*>(smem_raw);
-  cplx* wb = vb + 2 * kmax;
-  cplx* vpub = wb + 2 * kmax;          // v_j as published by the owner (index l: column j+1+l)
-  cplx* pown = vpub + kmax;            // p_i of the own rows (local index i / TD_CL)
-  cplx* stash = pown + 2 * own_cap;    // the owner's next reflector row (row j + 1), updated through step j - 1
-  double* scal = reinterpret_cast<double*>(stash + kmax);   // [0..1] cpart, [2..3] tau, [8..] reduction
+  cplx* vb = reinterpret_cast<cplx*>(smem_raw);   // v of two consecutive steps: vb + (j & 1) kmax
+  cplx* wb = vb + 2 * kmax;                        // w likewise
+  cplx* pub = wb + 2 * kmax;                       // row j + 1 as published by its owner
+  cplx* nrow = pub + kmax;                         // this CTA's copy of the row being reduced
+  cplx* pown = nrow + kmax;                        // p of the own rows: pown + (j & 1) own_cap
+  // [0..3] partial c of the two parities, [4..5] tau of this step, [8..] warp partials
+  double* scal = reinterpret_cast<double*>(pown + 2 * own_cap);
   const SectorDesc& S = sd[list[blockIdx.x / TD_CL]];
   const int k = S.k;                   // the same for every CTA of the cluster
   cplx* A = gbuf + S.g_off;
@@ -118,35 +123,34 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
     if (k == 1 && rank == 0 && tid == 0) dd[0] = A[0].x;
     return;                            // uniform over the cluster
   }
+  double beta = 0.0;                   // this step's e_j (warp 0)
   for (int j = 0; j < k - 1; ++j) {
-    const int t = k - j - 1;
-    const int owner = j % TD_CL;
-    cplx* vcur = vb + (j & 1) * kmax;
-    const cplx* vprev = vb + ((j + 1) & 1) * kmax;
-    const cplx* wprev = wb + ((j + 1) & 1) * kmax;
-    // ---- S0: the reflector of row j (one warp of the owner; warp shuffles only)
-    if (rank == owner && warp == 0) {
-      cplx* row = A + (int64_t)j * k;
+    const int par = j & 1;
+    const bool owner = rank == j % TD_CL;
+    cplx* vcur = vb + par * kmax;
+    const cplx* vprev = vb + (par ^ 1) * kmax;
+    const cplx* wprev = wb + (par ^ 1) * kmax;
+    // ---- R: the reflector of row j (warp 0 of every CTA; warp shuffles only)
+    if (warp == 0) {
+      const cplx* row = A + (int64_t)j * k;
       double part = 0.0;
       const cplx vj = j > 0 ? vprev[j] : cmake(0.0, 0.0), wj = j > 0 ? wprev[j] : cmake(0.0, 0.0);
       for (int l = j + lane; l < k; l += 32) {
-        // row j as the previous pass left it (kept in shared memory by this CTA), or the
-        // Gram itself at j = 0
-        cplx a = j > 0 ? stash[l] : ldc(row + l);
+        // row j as the previous pass left it (copied from its owner), the Gram at j = 0
+        cplx a = j > 0 ? nrow[l] : ldc(row + l);
         if (j > 0) a = csub(a, cadd(cmulc(vj, wprev[l]), cmulc(wj, vprev[l])));
         if (l == j) {
-          dd[j] = a.x;
+          if (owner) dd[j] = a.x;
         } else {
           const cplx x = cconj(a);
-          vpub[l - j - 1] = x;          // x for now, scaled below
+          vcur[l] = x;                  // x for now, scaled below
           if (l > j + 1) part += cabs2(x);
         }
       }
       const double xn2 = warp_sum(part);   // the same value in every lane
       __syncwarp();
-      const cplx alpha = vpub[0];
+      const cplx alpha = vcur[j + 1];
       cplx tau, sc;
-      double beta;
       if (xn2 == 0.0 && alpha.y == 0.0) {
         tau = cmake(0.0, 0.0);
         beta = alpha.x;
@@ -156,30 +160,21 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
         tau = cmake((beta - alpha.x) / beta, -alpha.y / beta);
         sc = cdiv(cmake(1.0, 0.0), cmake(alpha.x - beta, alpha.y));
       }
-      __syncwarp();                     // alpha read by every lane before vpub[0] changes
-      for (int l = lane; l < t; l += 32) {
-        const cplx v = l == 0 ? cmake(1.0, 0.0) : cmul(sc, vpub[l]);
-        vpub[l] = v;
-        stc(row + j + 1 + l, v);        // v_j kept in row j for the back-transformation
-      }
+      __syncwarp();                     // alpha read by every lane before vcur[j + 1] changes
+      for (int l = j + 1 + lane; l < k; l += 32)
+        vcur[l] = l == j + 1 ? cmake(1.0, 0.0) : cmul(sc, vcur[l]);
       if (lane == 0) {
-        ee[j] = beta;
-        tt[j] = tau;
-        scal[2] = tau.x;
-        scal[3] = tau.y;
+        scal[4] = tau.x;
+        scal[5] = tau.y;
       }
     }
-    cluster.sync();
-    // ---- S1: fused update + matrix-vector product on the own rows
+    __syncthreads();
+    const cplx tau = cmake(scal[4], scal[5]);
+    // ---- P: fused update + matrix-vector product on the own rows
     {
-      const cplx* rv = cluster.map_shared_rank(vpub, owner);
-      const double* rs = cluster.map_shared_rank(scal, owner);
-      for (int l = tid; l < t; l += TD_NT) vcur[j + 1 + l] = rv[l];
-      const cplx tau = cmake(rs[2], rs[3]);
-      __syncthreads();
-      // own rows i > j: first own row, then every TD_CL-th
       const int i0 = j + 1 + ((rank - (j + 1)) % TD_CL + TD_CL) % TD_CL;
       double cpx = 0.0, cpy = 0.0;
+      cplx* pw = pown + par * own_cap;
       // two rows per warp in flight (rows i and i + stride), so the loads of one hide
       // the latency of the other
       const int stride = TD_CL * (TD_NT / 32);
@@ -188,7 +183,7 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
         const bool two = i2 < k;       // warp-uniform
         cplx* row = A + (int64_t)i * k;
         cplx* row2 = A + (int64_t)(two ? i2 : i) * k;
-        const bool next = i == j + 1;  // the next reflector row: keep it in shared memory
+        const bool next = i == j + 1;  // the next reflector row: publish it
         const cplx vi = j > 0 ? vprev[i] : cmake(0.0, 0.0), wi = j > 0 ? wprev[i] : cmake(0.0, 0.0);
         const cplx vi2 = (j > 0 && two) ? vprev[i2] : cmake(0.0, 0.0);
         const cplx wi2 = (j > 0 && two) ? wprev[i2] : cmake(0.0, 0.0);
@@ -207,13 +202,13 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
               stc(row2 + l, a2);
             }
           }
-          if (next) stash[l] = a;
+          if (next) pub[l] = a;
           cfma(acc, a, vc);
           cfma(acc2, a2, vc);
         }
         acc = warp_sum(acc);
         const cplx p = cmul(tau, acc);
-        if (lane == 0) pown[i / TD_CL] = p;
+        if (lane == 0) pw[i / TD_CL] = p;
         // conj(p_i) v_i, summed by lane 0 of each warp in row order
         const cplx cv = ccmul(p, vcur[i]);
         cpx += cv.x;
@@ -221,7 +216,7 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
         if (two) {
           acc2 = warp_sum(acc2);
           const cplx p2 = cmul(tau, acc2);
-          if (lane == 0) pown[i2 / TD_CL] = p2;
+          if (lane == 0) pw[i2 / TD_CL] = p2;
           const cplx cv2 = ccmul(p2, vcur[i2]);
           cpx += cv2.x;
           cpy += cv2.y;
@@ -235,37 +230,45 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
       if (tid == 0) {
         double sx = 0.0, sy = 0.0;
         for (int w = 0; w < TD_NT / 32; ++w) { sx += scal[8 + 2 * w]; sy += scal[9 + 2 * w]; }
-        scal[0] = sx;
-        scal[1] = sy;
+        scal[2 * par] = sx;
+        scal[2 * par + 1] = sy;
       }
     }
     cluster.sync();
-    // ---- S2: c from the partials, then the whole w_j = p - tau c / 2 v, each CTA
-    // reading the p of every row from its owner (no further barrier: the next writes of
-    // pown and of the partials follow the next step's first barrier)
+    // ---- G: w_j from every owner's p, the next row from its owner
     {
-      const double* rs = cluster.map_shared_rank(scal, owner);
-      const cplx tau = cmake(rs[2], rs[3]);
       double cx = 0.0, cy = 0.0;
-      for (int q = 0; q < TD_CL; ++q) {   // fixed order
+      for (int q = 0; q < TD_CL; ++q) {   // fixed order: the same sum in every CTA
         const double* qs = cluster.map_shared_rank(scal, q);
-        cx += qs[0];
-        cy += qs[1];
+        cx += qs[2 * par];
+        cy += qs[2 * par + 1];
       }
       const cplx a2 = cscale(cmul(tau, cmake(cx, cy)), -0.5);
-      cplx* wcur = wb + (j & 1) * kmax;
+      cplx* wcur = wb + par * kmax;
+      const cplx* rpub = cluster.map_shared_rank(pub, (j + 1) % TD_CL);
       for (int l = j + 1 + tid; l < k; l += TD_NT) {
         const cplx* rp = cluster.map_shared_rank(pown, l % TD_CL);
-        wcur[l] = cadd(rp[l / TD_CL], cmul(a2, vcur[l]));
+        wcur[l] = cadd(rp[par * own_cap + l / TD_CL], cmul(a2, vcur[l]));
+        nrow[l] = rpub[l];
+      }
+      if (owner) {
+        // v_j kept in row j for the back-transformation (row j has been read by every
+        // CTA before the barrier)
+        cplx* row = A + (int64_t)j * k;
+        for (int l = j + 1 + tid; l < k; l += TD_NT) stc(row + l, vcur[l]);
+        if (tid == 0) {
+          ee[j] = beta;                 // thread 0 is lane 0 of warp 0, which formed it
+          tt[j] = tau;
+        }
       }
       __syncthreads();
     }
   }
-  // last diagonal entry: the update of step k - 2 on A[k-1][k-1]
+  // last diagonal entry: row k - 1 (copied in the last G) minus the update of step k - 2
   if (rank == (k - 1) % TD_CL && tid == 0) {
     const int j = k - 1;
     const cplx v = vb[((k - 2) & 1) * kmax + j], w = wb[((k - 2) & 1) * kmax + j];
-    const cplx a = csub(ldc(A + (int64_t)j * k + j), cadd(cmulc(v, w), cmulc(w, v)));
+    const cplx a = csub(nrow[j], cadd(cmulc(v, w), cmulc(w, v)));
     dd[j] = a.x;
   }
   cluster.sync();   // no CTA leaves while another may still read its shared memory
