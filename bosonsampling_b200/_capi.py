@@ -40,6 +40,7 @@ SIGNATURES = {
     "bsmpo_bs_update": (_c_int, [_vp, _c_int, _dp]),
     "bsmpo_bs_update_tensor": (_c_int, [_vp, _c_int, _vp]),
     "bsmpo_run_mesh": (_c_int, [_vp, _c_int, _ip, _dp, _dp]),
+    "bsmpo_run_mesh_host": (_c_int, [_vp, _c_int, _ip, _dp, _dp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bsmpo_mesh_truncation": (_c_int, [_vp, _dp, _c_int]),
     "bsmpo_apply_phases": (_c_int, [_vp, _dp]),
     "bsmpo_observables": (_c_int, [_vp, _dp, _dp]),

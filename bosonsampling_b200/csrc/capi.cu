@@ -101,6 +101,12 @@ struct bsmpo_ctx {
   // 1.1e-4 / 1.3e-3 marginal error on the N=16 / N=32 circuits against 8.7e-6 / 1.0e-4
   // with Theta alone)
   int tc_mask = 1;
+  // the tridiagonalisation's four size-class launches go on forked streams (1) or one
+  // after another on the update's stream (0); BSMPO_TD_FORK.  With concurrent updates the
+  // streams of all workers share the device's hardware queues
+  // (CUDA_DEVICE_MAX_CONNECTIONS, at most 32): streams beyond that count are serialised
+  // with others, so the fork pays only while workers x 4 stays within the queues
+  int td_fork = 1;
   HostStage stage, stage2, hres;
   // last update diagnostics (host)
   std::vector<int> last_cc, last_shape, last_kept, last_k;
@@ -146,6 +152,25 @@ int fail(bsmpo_ctx* h, int code, const std::string& msg) {
 std::vector<int>& mirror(bsmpo_ctx* h) { return h->cnt_shared ? *h->cnt_shared : h->cnt; }
 
 // waits (sleeping) until the handle's stream has drained
+// the forked streams of the tridiagonalisation's size classes and their events, created
+// once (for a worker when it is made, so the order of stream creation, which decides
+// the streams' hardware queues, is fixed)
+int make_fork_streams(bsmpo_ctx* h) {
+  if (h->fork_ev) return BSMPO_OK;
+  if (cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    h->fork_ev = nullptr;
+    return fail(h, BSMPO_ECUDA, "fork event creation failed");
+  }
+  for (int i = 0; i < 3; ++i)
+    if (cudaStreamCreateWithFlags(&h->aux[i], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->join_ev[i], cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(h, BSMPO_ECUDA, "fork stream creation failed");
+    }
+  return BSMPO_OK;
+}
+
 cudaError_t host_wait(bsmpo_ctx* h) {
   if (!h->wait_ev) {
     cudaError_t e = cudaEventCreateWithFlags(&h->wait_ev, cudaEventBlockingSync | cudaEventDisableTiming);
@@ -578,14 +603,13 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   const int* tdlist_d = reinterpret_cast<const int*>(dt + L.tdlist);
   const bool tc = h->precision == BSMPO_PRECISION_TF32X3;
   const bool tc_theta = tc && (h->tc_mask & 1), tc_w = tc && (h->tc_mask & 2);
-  int* tcerr_d = nullptr;
-  if (tc) {
-    if (!h->tcerr.p) {
-      if ((rc = grow(h, h->tcerr, sizeof(int)))) return rc;
-      CK(h, cudaMemsetAsync(h->tcerr.p, 0, sizeof(int), st));
-    }
-    tcerr_d = reinterpret_cast<int*>(h->tcerr.p);
+  // error word of the asynchronous pipelines (tensor-core GEMM, streamed
+  // tridiagonalisation): set on the device when a bounded wait expires
+  if (!h->tcerr.p) {
+    if ((rc = grow(h, h->tcerr, sizeof(int)))) return rc;
+    CK(h, cudaMemsetAsync(h->tcerr.p, 0, sizeof(int), st));
   }
+  int* tcerr_d = reinterpret_cast<int*>(h->tcerr.p);
   // The Gram route drops singular values below ~2e-6 of a sector's largest.  Where the
   // update does not truncate to chi that is pure loss (W = V^H C carries them through
   // 1 / Lambda_R), so such updates take the exact Jacobi SVD: up front when the
@@ -642,14 +666,9 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
     CKL(h, launch_zgemm_grouped(h->abuf.p, h->abuf.p, h->gbuf.p, nullptr, ggram_d, (int)P.ggram.size(),
                                 P.gram_tiles, st));
     {
-      if (!h->fork_ev) {
-        CK(h, cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
-        for (int i = 0; i < 3; ++i) {
-          CK(h, cudaStreamCreateWithFlags(&h->aux[i], cudaStreamNonBlocking));
-          CK(h, cudaEventCreateWithFlags(&h->join_ev[i], cudaEventDisableTiming));
-        }
-      }
-      const cudaStream_t ts[4] = {st, h->aux[0], h->aux[1], h->aux[2]};
+      const bool fork = h->td_fork != 0;
+      if (fork && (rc = make_fork_streams(h))) return rc;
+      const cudaStream_t ts[4] = {st, fork ? h->aux[0] : st, fork ? h->aux[1] : st, fork ? h->aux[2] : st};
       if (h->timing) {
         if (!h->td_ev0) {
           CK(h, cudaEventCreate(&h->td_ev0));
@@ -657,11 +676,14 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
         }
         CK(h, cudaEventRecord(h->td_ev0, st));
       }
-      CK(h, cudaEventRecord(h->fork_ev, st));
-      for (int i = 0; i < 3; ++i)
-        if (P.td_count[2 - i] > 0) CK(h, cudaStreamWaitEvent(h->aux[i], h->fork_ev, 0));
-      CK(h, launch_tridiag(sd_d, tdlist_d, P.td_count, P.td_kmax, h->gbuf.p, dbuf_d, ebuf_d, h->taub.p, ts));
-      for (int i = 0; i < 3; ++i)
+      if (fork) {
+        CK(h, cudaEventRecord(h->fork_ev, st));
+        for (int i = 0; i < 3; ++i)
+          if (P.td_count[2 - i] > 0) CK(h, cudaStreamWaitEvent(h->aux[i], h->fork_ev, 0));
+      }
+      CK(h, launch_tridiag(sd_d, tdlist_d, P.td_count, P.td_kmax, h->gbuf.p, dbuf_d, ebuf_d, h->taub.p,
+                           tcerr_d, ts));
+      for (int i = 0; i < 3 && fork; ++i)
         if (P.td_count[2 - i] > 0) {
           CK(h, cudaEventRecord(h->join_ev[i], h->aux[i]));
           CK(h, cudaStreamWaitEvent(st, h->join_ev[i], 0));
@@ -806,10 +828,10 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
   CK(h, cudaMemcpyAsync(hk, kept_d, (size_t)(ns + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(h, cudaMemcpyAsync(htw, trunc_d, sizeof(double), cudaMemcpyDeviceToHost, st));
   int* htc = reinterpret_cast<int*>(static_cast<char*>(h->hres.p) + 1000);
-  if (tc) CK(h, cudaMemcpyAsync(htc, tcerr_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(h, cudaMemcpyAsync(htc, tcerr_d, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(h, host_wait(h));
-  if (tc && *htc != 0)
-    return fail(h, BSMPO_ECUDA, "tensor-core GEMM: a pipeline wait expired (error word set)");
+  if (*htc != 0)
+    return fail(h, BSMPO_ECUDA, "tensor-core GEMM or tridiagonalisation: a pipeline wait expired (error word set)");
   total_kept = hk[ns];
   if (gram && total_kept < chi && h->cutoff == 0.0 && h->gram_policy >= 1) {
     // not truncated to chi: redo the SVD exactly (the Gram matrix and the eigen buffers
@@ -1045,6 +1067,8 @@ void free_workspaces(bsmpo_ctx* h) {
   }
 }
 
+void destroy_worker(bsmpo_ctx* w);
+
 // A worker context for concurrent updates: the owner's state, its own stream.
 int make_worker(bsmpo_ctx* h, bsmpo_ctx** out) {
   bsmpo_ctx* w = new bsmpo_ctx();
@@ -1054,10 +1078,16 @@ int make_worker(bsmpo_ctx* h, bsmpo_ctx** out) {
   w->loaded = true;
   w->cnt_shared = &h->cnt;
   w->profile = h->profile;
+  w->td_fork = h->td_fork;
   if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
     delete w;
     return fail(h, BSMPO_ECUDA, "worker stream creation failed");
+  }
+  if (w->td_fork && make_fork_streams(w) != BSMPO_OK) {
+    const std::string msg = w->err;
+    destroy_worker(w);
+    return fail(h, BSMPO_ECUDA, msg);
   }
   *out = w;
   return BSMPO_OK;
@@ -1078,7 +1108,22 @@ void destroy_worker(bsmpo_ctx* w) {
 // host mirror entries are written; device side: the worker's stream waits for the
 // events recorded at their ends), so consecutive brick-wall layers overlap.  Every
 // update computes exactly what it computes alone.
-int run_mesh_concurrent(bsmpo_ctx* h, int n_bs, const int* modes, const cplx* u3, int nw) {
+// The host side of a mesh over a host-resident state: the first update touching site s,
+// first[s], copies the site in on its own stream before it starts, and the last, last[s],
+// copies it out after it ends.  Every later update touching the site depends on the
+// first one (they share a site), and the last one on every earlier one, so the copies
+// need no events of their own; they run in the workers' streams, where they overlap the
+// other workers' updates without extra streams (which would share the device's hardware
+// queues with the workers' streams).
+struct HostStream {
+  std::vector<int> first, last;
+  const char* gamma_in = nullptr;
+  char* gamma_out = nullptr;
+  size_t site_bytes = 0;
+};
+
+int run_mesh_concurrent(bsmpo_ctx* h, int n_bs, const int* modes, const cplx* u3, int nw,
+                        HostStream* hs = nullptr) {
   const int d3 = h->d * h->d * h->d;
   int rc;
   while ((int)h->workers.size() < nw) {
@@ -1092,6 +1137,7 @@ int run_mesh_concurrent(bsmpo_ctx* h, int n_bs, const int* modes, const cplx* u3
     w->precision = h->precision;
     w->gram_policy = h->gram_policy;
     w->tc_mask = h->tc_mask;
+    w->td_fork = h->td_fork;
     w->jac_rows = h->jac_rows;
     w->timing = h->timing;
     if (w->timing && !w->ev0) {
@@ -1153,10 +1199,23 @@ int run_mesh_concurrent(bsmpo_ctx* h, int n_bs, const int* modes, const cplx* u3
           if (j >= 0 && cudaStreamWaitEvent(w->stream, done_ev[j], 0) != cudaSuccess)
             r = fail(w, BSMPO_ECUDA, "cudaStreamWaitEvent failed");
         }
+        for (int site = modes[k]; hs && site <= modes[k] + 1 && !r; ++site)
+          if (hs->first[site] == k &&
+              cudaMemcpyAsync(reinterpret_cast<char*>(h->gamma) + (size_t)site * hs->site_bytes,
+                              hs->gamma_in + (size_t)site * hs->site_bytes, hs->site_bytes,
+                              cudaMemcpyHostToDevice, w->stream) != cudaSuccess)
+            r = fail(w, BSMPO_ECUDA, "site copy-in failed");
         if (!r) r = bs_update_impl(w, modes[k], u3 + (size_t)k * d3);
         if (!r) h->mesh_tw[k] = w->last_trunc;   // each k is written by one worker only
         if (!r && cudaEventRecord(done_ev[k], w->stream) != cudaSuccess)
           r = fail(w, BSMPO_ECUDA, "cudaEventRecord failed");
+        for (int site = modes[k]; hs && site <= modes[k] + 1 && !r; ++site)
+          // the site's final value of this mesh: copied out behind the update
+          if (hs->last[site] == k &&
+              cudaMemcpyAsync(hs->gamma_out + (size_t)site * hs->site_bytes,
+                              reinterpret_cast<const char*>(h->gamma) + (size_t)site * hs->site_bytes,
+                              hs->site_bytes, cudaMemcpyDeviceToHost, w->stream) != cudaSuccess)
+            r = fail(w, BSMPO_ECUDA, "site copy-out failed");
         std::lock_guard<std::mutex> lock(mu);
         if (r) {
           if (!err_code) { err_code = r; err_msg = w->err; }
@@ -1369,6 +1428,8 @@ int bsmpo_create(int n, int d, int chi, int flags, bsmpo_ctx** out) {
   if (tm && tm[0] >= '0' && tm[0] <= '3') h->tc_mask = tm[0] - '0';
   const char* gp = std::getenv("BSMPO_GRAM_POLICY");
   if (gp && gp[0] >= '0' && gp[0] <= '2') h->gram_policy = gp[0] - '0';
+  const char* tf = std::getenv("BSMPO_TD_FORK");
+  if (tf && (tf[0] == '0' || tf[0] == '1')) h->td_fork = tf[0] - '0';
   const char* nwk = std::getenv("BSMPO_WORKERS");
   if (nwk && std::atoi(nwk) >= 1 && std::atoi(nwk) <= 64) h->n_workers = std::atoi(nwk);
   *out = h;
@@ -1416,23 +1477,14 @@ int bsmpo_set_cutoff(bsmpo_ctx* h, double cutoff) {
   return BSMPO_OK;
 }
 
-int bsmpo_load_state(bsmpo_ctx* h, const void* gamma, const double* lambda, const int* charge) {
-  if (!h || !gamma || !lambda || !charge) return fail(h, BSMPO_EINVAL, "null argument");
+}  // extern "C"
+
+// Validates the charges and Lambda of a state (host copies: hc [(n+1) chi][2], hl
+// [(n+1) chi] with the inner bonds filled) and rebuilds the host mirror of the block
+// sizes; fills the edge Lambda of hl (1 on the occupied slots of bonds 0 and n).
+int validate_state(bsmpo_ctx* h, const int* hc, double* hl) {
   const int n = h->n, d = h->d, chi = h->chi;
-  cudaStream_t st = h->stream;
-  CK(h, cudaMemcpyAsync(h->gamma, gamma, (size_t)n * chi * chi * sizeof(cplx),
-                        cudaMemcpyDeviceToDevice, st));
-  CK(h, cudaMemcpyAsync(h->lam + chi, lambda, (size_t)(n - 1) * chi * sizeof(double),
-                        cudaMemcpyDeviceToDevice, st));
-  CK(h, cudaMemcpyAsync(h->charge, charge, (size_t)(n + 1) * chi * 2 * sizeof(int),
-                        cudaMemcpyDeviceToDevice, st));
-  std::vector<int> hc((size_t)(n + 1) * chi * 2);
-  std::vector<double> hl((size_t)(n + 1) * chi, 0.0);
-  CK(h, cudaMemcpyAsync(hc.data(), charge, hc.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
-  CK(h, cudaMemcpyAsync(hl.data() + chi, lambda, (size_t)(n - 1) * chi * sizeof(double),
-                        cudaMemcpyDeviceToHost, st));
-  CK(h, cudaStreamSynchronize(st));
-  // validate: sorted, occupied slots first, charges in range, Lambda > 0 on occupied slots
+  // sorted, occupied slots first, charges in range, Lambda > 0 on occupied slots
   std::fill(h->cnt.begin(), h->cnt.end(), 0);
   for (int b = 0; b <= n; ++b) {
     bool empty_seen = false;
@@ -1458,9 +1510,32 @@ int bsmpo_load_state(bsmpo_ctx* h, const void* gamma, const double* lambda, cons
       h->cnt[(size_t)b * d * d + c0 * d + c1]++;
     }
   }
-  // edge Lambda: 1 on occupied slots of bonds 0 and n
   for (int b : {0, n})
     for (int i = 0; i < chi; ++i) hl[(size_t)b * chi + i] = hc[((size_t)b * chi + i) * 2] < d ? 1.0 : 0.0;
+  return BSMPO_OK;
+}
+
+extern "C" {
+
+int bsmpo_load_state(bsmpo_ctx* h, const void* gamma, const double* lambda, const int* charge) {
+  if (!h || !gamma || !lambda || !charge) return fail(h, BSMPO_EINVAL, "null argument");
+  const int n = h->n, chi = h->chi;
+  cudaStream_t st = h->stream;
+  h->loaded = false;
+  CK(h, cudaMemcpyAsync(h->gamma, gamma, (size_t)n * chi * chi * sizeof(cplx),
+                        cudaMemcpyDeviceToDevice, st));
+  CK(h, cudaMemcpyAsync(h->lam + chi, lambda, (size_t)(n - 1) * chi * sizeof(double),
+                        cudaMemcpyDeviceToDevice, st));
+  CK(h, cudaMemcpyAsync(h->charge, charge, (size_t)(n + 1) * chi * 2 * sizeof(int),
+                        cudaMemcpyDeviceToDevice, st));
+  std::vector<int> hc((size_t)(n + 1) * chi * 2);
+  std::vector<double> hl((size_t)(n + 1) * chi, 0.0);
+  CK(h, cudaMemcpyAsync(hc.data(), charge, hc.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(h, cudaMemcpyAsync(hl.data() + chi, lambda, (size_t)(n - 1) * chi * sizeof(double),
+                        cudaMemcpyDeviceToHost, st));
+  CK(h, cudaStreamSynchronize(st));
+  int rc = validate_state(h, hc.data(), hl.data());
+  if (rc) return rc;
   CK(h, cudaMemcpyAsync(h->lam, hl.data(), chi * sizeof(double), cudaMemcpyHostToDevice, st));
   CK(h, cudaMemcpyAsync(h->lam + (size_t)n * chi, hl.data() + (size_t)n * chi, chi * sizeof(double),
                         cudaMemcpyHostToDevice, st));
@@ -1562,15 +1637,16 @@ int bsmpo_bs_update(bsmpo_ctx* h, int mode, const double* S) {
   return bs_update_impl(h, mode, reinterpret_cast<const cplx*>(h->u3.p));
 }
 
-int bsmpo_run_mesh(bsmpo_ctx* h, int n_bs, const int* modes, const double* theta, const double* phi) {
-  if (!h || n_bs < 0 || (n_bs > 0 && (!modes || !theta || !phi))) return fail(h, BSMPO_EINVAL, "bad argument");
-  if (!h->loaded) return fail(h, BSMPO_EINVAL, "no state loaded");
+}  // extern "C"
+
+// A mesh of beam splitters (T(theta, phi) each) on the loaded state; with hs, over the
+// host-resident state whose sites are arriving (see HostStream).
+int run_mesh_impl(bsmpo_ctx* h, int n_bs, const int* modes, const double* theta, const double* phi,
+                  HostStream* hs) {
   h->mesh_tw.assign(n_bs, 0.0);
   if (n_bs == 0) return BSMPO_OK;
   const int d = h->d, d3 = d * d * d;
   int rc;
-  for (int i = 0; i < n_bs; ++i)
-    if (modes[i] < 0 || modes[i] > h->n - 2) return fail(h, BSMPO_EINVAL, "mode out of range");
   if ((rc = grow(h, h->u3, (size_t)n_bs * d3 * sizeof(cplx)))) return rc;
   if ((rc = grow(h, h->m4, (size_t)n_bs * 8 * sizeof(double)))) return rc;
   std::vector<double> m4((size_t)n_bs * 8);
@@ -1589,13 +1665,81 @@ int bsmpo_run_mesh(bsmpo_ctx* h, int n_bs, const int* modes, const double* theta
   // the stage is reused by the updates, and worker streams read u3: drain the stream
   CK(h, cudaStreamSynchronize(h->stream));
   const int nw = std::min(h->n_workers, n_bs);
-  if (nw > 1) return run_mesh_concurrent(h, n_bs, modes, reinterpret_cast<const cplx*>(h->u3.p), nw);
+  if (nw > 1 || hs)
+    return run_mesh_concurrent(h, n_bs, modes, reinterpret_cast<const cplx*>(h->u3.p), std::max(nw, 1), hs);
   h->diag = nullptr;
   for (int i = 0; i < n_bs; ++i) {
     rc = bs_update_impl(h, modes[i], reinterpret_cast<const cplx*>(h->u3.p) + (size_t)i * d3);
     if (rc) return rc;
     h->mesh_tw[i] = h->last_trunc;
   }
+  return BSMPO_OK;
+}
+
+int check_mesh_args(bsmpo_ctx* h, int n_bs, const int* modes, const double* theta, const double* phi) {
+  if (!h || n_bs < 0 || (n_bs > 0 && (!modes || !theta || !phi))) return fail(h, BSMPO_EINVAL, "bad argument");
+  for (int i = 0; i < n_bs; ++i)
+    if (modes[i] < 0 || modes[i] > h->n - 2) return fail(h, BSMPO_EINVAL, "mode out of range");
+  return BSMPO_OK;
+}
+
+extern "C" {
+
+int bsmpo_run_mesh(bsmpo_ctx* h, int n_bs, const int* modes, const double* theta, const double* phi) {
+  int rc = check_mesh_args(h, n_bs, modes, theta, phi);
+  if (rc) return rc;
+  if (!h->loaded) return fail(h, BSMPO_EINVAL, "no state loaded");
+  return run_mesh_impl(h, n_bs, modes, theta, phi, nullptr);
+}
+
+int bsmpo_run_mesh_host(bsmpo_ctx* h, int n_bs, const int* modes, const double* theta, const double* phi,
+                        const void* gamma_in, const double* lambda_in, const int* charge_in, void* gamma_out,
+                        double* lambda_out, int* charge_out) {
+  int rc = check_mesh_args(h, n_bs, modes, theta, phi);
+  if (rc) return rc;
+  if (!gamma_in || !lambda_in || !charge_in || !gamma_out || !lambda_out || !charge_out)
+    return fail(h, BSMPO_EINVAL, "null argument");
+  const int n = h->n, chi = h->chi;
+  const size_t site_bytes = (size_t)chi * chi * sizeof(cplx);
+  cudaStream_t st = h->stream;
+  h->loaded = false;
+  // the bonds: validated on the host, copied in before any site
+  std::vector<double> hl((size_t)(n + 1) * chi, 0.0);
+  std::memcpy(hl.data() + chi, lambda_in, (size_t)(n - 1) * chi * sizeof(double));
+  if ((rc = validate_state(h, charge_in, hl.data()))) return rc;
+  CK(h, cudaMemcpyAsync(h->lam, hl.data(), hl.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(h, cudaMemcpyAsync(h->charge, charge_in, (size_t)(n + 1) * chi * 2 * sizeof(int), cudaMemcpyHostToDevice, st));
+  CK(h, cudaStreamSynchronize(st));
+  h->loaded = true;
+  HostStream hs;
+  hs.first.assign(n, -1);
+  hs.last.assign(n, -1);
+  hs.gamma_in = static_cast<const char*>(gamma_in);
+  hs.gamma_out = static_cast<char*>(gamma_out);
+  hs.site_bytes = site_bytes;
+  for (int k = n_bs - 1; k >= 0; --k) hs.first[modes[k]] = hs.first[modes[k] + 1] = k;
+  for (int k = 0; k < n_bs; ++k) hs.last[modes[k]] = hs.last[modes[k] + 1] = k;
+  // the sites no update touches: in and straight out on the handle's stream
+  for (int s = 0; s < n; ++s)
+    if (hs.first[s] < 0) {
+      CK(h, cudaMemcpyAsync(reinterpret_cast<char*>(h->gamma) + (size_t)s * site_bytes,
+                            hs.gamma_in + (size_t)s * site_bytes, site_bytes, cudaMemcpyHostToDevice, st));
+      CK(h, cudaMemcpyAsync(hs.gamma_out + (size_t)s * site_bytes,
+                            reinterpret_cast<const char*>(h->gamma) + (size_t)s * site_bytes, site_bytes,
+                            cudaMemcpyDeviceToHost, st));
+    }
+  rc = run_mesh_impl(h, n_bs, modes, theta, phi, &hs);
+  if (rc) {
+    cudaStreamSynchronize(st);
+    h->loaded = false;   // the device state is incomplete
+    return rc;
+  }
+  // the bonds, once every update has finished (the workers are drained)
+  CK(h, cudaMemcpyAsync(lambda_out, h->lam + chi, (size_t)(n - 1) * chi * sizeof(double), cudaMemcpyDeviceToHost,
+                        st));
+  CK(h, cudaMemcpyAsync(charge_out, h->charge, (size_t)(n + 1) * chi * 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                        st));
+  CK(h, cudaStreamSynchronize(st));
   return BSMPO_OK;
 }
 

@@ -28,6 +28,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "pipeline.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -48,10 +49,31 @@ constexpr double EPS = 2.220446049250313e-16;
 constexpr int TD_NT = BSMPO_TD_NT;
 constexpr int TD_CLASSES = 4;   // cluster sizes 1, 2, 4, 8 CTAs per sector, by sector size
 
-// dynamic shared memory of the tridiagonalisation (kmax = largest k of the launch)
+constexpr int TD_NW = TD_NT / 32;   // warps per CTA, each streaming its own rows
+// bulk-copy ring of each warp: about BSMPO_TD_RING_KB per CTA, 2 to TD_MAXSLOT row slots
+// (pairs of rows share one pass over the vectors), 1 above k = 768 (shared memory)
+#ifndef BSMPO_TD_RING_KB
+#define BSMPO_TD_RING_KB 64
+#endif
+constexpr int TD_MAXSLOT = 4;
+#ifndef BSMPO_TD_PAIRS
+#define BSMPO_TD_PAIRS 1   // rows two at a time (0: one at a time)
+#endif
+static_assert(TD_NW >= 1 && TD_NW <= 8, "the per-warp scalars of the tridiagonalisation hold 8 warps");
+
+__host__ __device__ inline int td_slots(int kmax) {
+  if (kmax > 768) return 1;
+  const long long s = (long long)BSMPO_TD_RING_KB * 1024 / ((long long)TD_NW * kmax * (long long)sizeof(cplx));
+  return (int)(s < 2 ? 2 : (s > TD_MAXSLOT ? TD_MAXSLOT : s));
+}
+
+// dynamic shared memory of the tridiagonalisation (kmax = largest k of the launch): the
+// row rings, v and w of two steps, the published and the copied row, p of the own rows
+// (two steps), 64 scalars and the rings' mbarriers
 __host__ __device__ inline size_t td_smem_bytes(int kmax, int cl) {
   const int own = kmax / cl + 1;
-  return sizeof(cplx) * ((size_t)6 * kmax + 2 * (size_t)own) + 64 * sizeof(double);
+  return sizeof(cplx) * ((size_t)TD_NW * td_slots(kmax) * kmax + 6 * (size_t)kmax + 2 * (size_t)own) +
+         64 * sizeof(double) + TD_NW * TD_MAXSLOT * sizeof(uint64_t);
 }
 
 __device__ __forceinline__ cplx warp_sum(cplx v) {
@@ -67,6 +89,19 @@ __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
+}
+
+// a - (x conj(y) + u conj(z)), eight fused multiply-adds (the rank-2 update of one entry)
+__device__ __forceinline__ cplx crank2(cplx a, cplx x, cplx y, cplx u, cplx z) {
+  a.x = fma(-x.x, y.x, a.x);
+  a.x = fma(-x.y, y.y, a.x);
+  a.x = fma(-u.x, z.x, a.x);
+  a.x = fma(-u.y, z.y, a.x);
+  a.y = fma(-x.y, y.x, a.y);
+  a.y = fma(x.x, y.y, a.y);
+  a.y = fma(-u.y, z.x, a.y);
+  a.y = fma(u.x, z.y, a.y);
+  return a;
 }
 
 // a / b for complex b != 0
@@ -95,24 +130,36 @@ __device__ __forceinline__ cplx cdiv(cplx a, cplx b) {
 //    p and the partials are double-buffered by step parity; the published row is written
 //    again only cl steps later: every next write follows the next barrier, which no CTA
 //    passes before every CTA has finished its G.
-// Every row of the trailing matrix is read and written by its owner only.
+//    Rows stream through shared memory.  Warp w of a CTA handles its own rows number
+//    r = w (mod 4) in every step (row i = rank + r cl), through a private ring of row
+//    slots: its lane 0 issues a bulk copy (cp.async.bulk, completion counted on the
+//    slot's mbarrier) of the row's trailing segment as soon as the slot is free and the
+//    warp has written that row back in the previous step, so the copies run ahead of
+//    the pass -- across the barrier, G and the next R into the next step's first rows
+//    -- instead of one L2 round trip per load.  A row is read and written by one warp
+//    only; its write-back is ordered before the next bulk read of it by a proxy fence
+//    of the writing lanes and the warp's synchronisation.
 __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
     tridiag_kernel(const SectorDesc* __restrict__ sd, const int* __restrict__ list, int kmax,
                    cplx* __restrict__ gbuf, double* __restrict__ dbuf, double* __restrict__ ebuf,
-                   cplx* __restrict__ taubuf) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+                   cplx* __restrict__ taubuf, int* __restrict__ err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
   const int TD_CL = (int)cluster.num_blocks();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int own_cap = kmax / TD_CL + 1;
-  cplx* vb = reinterpret_cast<cplx*>(smem_raw);   // v of two consecutive steps: vb + (j & 1) kmax
+  const int nslot = td_slots(kmax);
+  cplx* ring = reinterpret_cast<cplx*>(smem_raw);  // slot s of warp w: ring + (w nslot + s) kmax
+  cplx* vb = ring + (size_t)TD_NW * nslot * kmax;  // v of two consecutive steps: vb + (j & 1) kmax
   cplx* wb = vb + 2 * kmax;                        // w likewise
   cplx* pub = wb + 2 * kmax;                       // row j + 1 as published by its owner
   cplx* nrow = pub + kmax;                         // this CTA's copy of the row being reduced
   cplx* pown = nrow + kmax;                        // p of the own rows: pown + (j & 1) own_cap
   // [0..3] partial c of the two parities, [4..5] tau of this step, [8..] warp partials
   double* scal = reinterpret_cast<double*>(pown + 2 * own_cap);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(scal + 64) + warp * TD_MAXSLOT;   // this warp's
+  cplx* wring = ring + (size_t)warp * nslot * kmax;
   const SectorDesc& S = sd[list[blockIdx.x / TD_CL]];
   const int k = S.k;                   // the same for every CTA of the cluster
   cplx* A = gbuf + S.g_off;
@@ -123,6 +170,41 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
     if (k == 1 && rank == 0 && tid == 0) dd[0] = A[0].x;
     return;                            // uniform over the cluster
   }
+  if (lane < TD_MAXSLOT) {
+    mbar_init(bars + lane, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  // ---- this warp's row sequence: (step s, own row r) with rows i = rank + r cl > s,
+  // r = warp (mod 4), in step order, then row order; copies are issued in the same order
+  // as the pass consumes them, element q into slot q mod nslot
+  auto first_row = [&](int s) {
+    const int r0 = s >= rank ? (s - rank) / TD_CL + 1 : 0;
+    return r0 + ((warp - r0) % TD_NW + TD_NW) % TD_NW;
+  };
+  int is = 0, ir = first_row(0);       // next element to copy
+  int issued = 0, done = 0;            // elements copied / consumed
+  int ls = -1, lr = 0;                 // the last consumed element
+  auto issue = [&]() {
+    // a free slot, and the row's write-back of the previous step done (consumption is in
+    // sequence order, so the last consumed element tells)
+    while (is < k - 1 && rank + ir * TD_CL < k && issued < done + nslot &&
+           (is == 0 || ls > is - 1 || (ls == is - 1 && lr >= ir))) {
+      if (lane == 0) {
+        const int slot = issued % nslot;
+        const uint32_t bytes = (uint32_t)(k - is - 1) * (uint32_t)sizeof(cplx);
+        mbar_expect_tx(bars + slot, bytes);
+        bulk_load(wring + (size_t)slot * kmax, A + (int64_t)(rank + ir * TD_CL) * k + is + 1, bytes,
+                  bars + slot);
+      }
+      ++issued;
+      ir += TD_NW;
+      if (rank + ir * TD_CL >= k) ir = first_row(++is);
+    }
+  };
+  issue();
+
   double beta = 0.0;                   // this step's e_j (warp 0)
   for (int j = 0; j < k - 1; ++j) {
     const int par = j & 1;
@@ -138,7 +220,7 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
       for (int l = j + lane; l < k; l += 32) {
         // row j as the previous pass left it (copied from its owner), the Gram at j = 0
         cplx a = j > 0 ? nrow[l] : ldc(row + l);
-        if (j > 0) a = csub(a, cadd(cmulc(vj, wprev[l]), cmulc(wj, vprev[l])));
+        if (j > 0) a = crank2(a, vj, ldc(wprev + l), wj, ldc(vprev + l));
         if (l == j) {
           if (owner) dd[j] = a.x;
         } else {
@@ -170,45 +252,52 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
     }
     __syncthreads();
     const cplx tau = cmake(scal[4], scal[5]);
-    // ---- P: fused update + matrix-vector product on the own rows
+    // ---- P: fused update + matrix-vector product on this warp's rows
     {
-      const int i0 = j + 1 + ((rank - (j + 1)) % TD_CL + TD_CL) % TD_CL;
       double cpx = 0.0, cpy = 0.0;
       cplx* pw = pown + par * own_cap;
-      // two rows per warp in flight (rows i and i + stride), so the loads of one hide
-      // the latency of the other
-      const int stride = TD_CL * (TD_NT / 32);
-      for (int i = i0 + warp * TD_CL; i < k; i += 2 * stride) {
-        const int i2 = i + stride;
-        const bool two = i2 < k;       // warp-uniform
-        cplx* row = A + (int64_t)i * k;
-        cplx* row2 = A + (int64_t)(two ? i2 : i) * k;
-        const bool next = i == j + 1;  // the next reflector row: publish it
+      // rows two at a time where the ring holds two slots: one pass over the vectors for
+      // both rows
+      for (int r = first_row(j); rank + r * TD_CL < k;) {
+        const int r2 = r + TD_NW;
+        const int i = rank + r * TD_CL, i2 = rank + r2 * TD_CL;
+        const bool two = BSMPO_TD_PAIRS && nslot >= 2 && i2 < k;   // warp-uniform
+        const int slot = done % nslot, slot2 = (done + 1) % nslot;
+        // on expiry the error word is set and the pass goes on with what the slot holds
+        mbar_wait(bars + slot, (uint32_t)(done / nslot) & 1u, err);
+        if (two) mbar_wait(bars + slot2, (uint32_t)((done + 1) / nslot) & 1u, err);
+        const cplx* srow = wring + (size_t)slot * kmax - (j + 1);     // srow[l], l > j
+        const cplx* srow2 = wring + (size_t)slot2 * kmax - (j + 1);
+        cplx* grow = A + (int64_t)i * k;
+        cplx* grow2 = A + (int64_t)(two ? i2 : i) * k;
+        const bool next = i == j + 1;  // the next reflector row (never the second): publish it
         const cplx vi = j > 0 ? vprev[i] : cmake(0.0, 0.0), wi = j > 0 ? wprev[i] : cmake(0.0, 0.0);
         const cplx vi2 = (j > 0 && two) ? vprev[i2] : cmake(0.0, 0.0);
         const cplx wi2 = (j > 0 && two) ? wprev[i2] : cmake(0.0, 0.0);
         cplx acc = cmake(0.0, 0.0), acc2 = cmake(0.0, 0.0);
 #pragma unroll 2
         for (int l = j + 1 + lane; l < k; l += 32) {
-          cplx a = ldc(row + l);
-          cplx a2 = two ? ldc(row2 + l) : cmake(0.0, 0.0);
-          const cplx vc = vcur[l];
+          cplx a = ldc(srow + l);
+          cplx a2 = two ? ldc(srow2 + l) : cmake(0.0, 0.0);
+          const cplx vc = ldc(vcur + l);
           if (j > 0) {
-            const cplx vp = vprev[l], wp = wprev[l];
-            a = csub(a, cadd(cmulc(vi, wp), cmulc(wi, vp)));
-            stc(row + l, a);
+            const cplx vp = ldc(vprev + l), wp = ldc(wprev + l);
+            a = crank2(a, vi, wp, wi, vp);
+            stc(grow + l, a);
             if (two) {
-              a2 = csub(a2, cadd(cmulc(vi2, wp), cmulc(wi2, vp)));
-              stc(row2 + l, a2);
+              a2 = crank2(a2, vi2, wp, wi2, vp);
+              stc(grow2 + l, a2);
             }
           }
           if (next) pub[l] = a;
           cfma(acc, a, vc);
           cfma(acc2, a2, vc);
         }
+        // the write-back before the next bulk read of these rows (async proxy)
+        if (j > 0) asm volatile("fence.proxy.async.global;" ::: "memory");
         acc = warp_sum(acc);
         const cplx p = cmul(tau, acc);
-        if (lane == 0) pw[i / TD_CL] = p;
+        if (lane == 0) pw[r] = p;
         // conj(p_i) v_i, summed by lane 0 of each warp in row order
         const cplx cv = ccmul(p, vcur[i]);
         cpx += cv.x;
@@ -216,11 +305,17 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
         if (two) {
           acc2 = warp_sum(acc2);
           const cplx p2 = cmul(tau, acc2);
-          if (lane == 0) pw[i2 / TD_CL] = p2;
+          if (lane == 0) pw[r2] = p2;
           const cplx cv2 = ccmul(p2, vcur[i2]);
           cpx += cv2.x;
           cpy += cv2.y;
         }
+        __syncwarp();                  // every lane done with the slots and the rows
+        done += two ? 2 : 1;
+        ls = j;
+        lr = two ? r2 : r;
+        issue();
+        r = two ? r2 + TD_NW : r2;
       }
       if (lane == 0) {
         scal[8 + 2 * warp] = cpx;
@@ -229,7 +324,7 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
       __syncthreads();
       if (tid == 0) {
         double sx = 0.0, sy = 0.0;
-        for (int w = 0; w < TD_NT / 32; ++w) { sx += scal[8 + 2 * w]; sy += scal[9 + 2 * w]; }
+        for (int w = 0; w < TD_NW; ++w) { sx += scal[8 + 2 * w]; sy += scal[9 + 2 * w]; }
         scal[2 * par] = sx;
         scal[2 * par + 1] = sy;
       }
@@ -253,7 +348,7 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
       }
       if (owner) {
         // v_j kept in row j for the back-transformation (row j has been read by every
-        // CTA before the barrier)
+        // CTA before the barrier, and no copy of it is issued after step j - 1)
         cplx* row = A + (int64_t)j * k;
         for (int l = j + 1 + tid; l < k; l += TD_NT) stc(row + l, vcur[l]);
         if (tid == 0) {
@@ -268,7 +363,7 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
   if (rank == (k - 1) % TD_CL && tid == 0) {
     const int j = k - 1;
     const cplx v = vb[((k - 2) & 1) * kmax + j], w = wb[((k - 2) & 1) * kmax + j];
-    const cplx a = csub(nrow[j], cadd(cmulc(v, w), cmulc(w, v)));
+    const cplx a = crank2(nrow[j], v, w, w, v);
     dd[j] = a.x;
   }
   cluster.sync();   // no CTA leaves while another may still read its shared memory
@@ -576,11 +671,17 @@ __global__ __launch_bounds__(BT_NT) void backtransform_kernel(const SectorDesc* 
 }  // namespace
 
 int eigen_max_k() {
-  // shared memory of the tridiagonalisation: (6 k + 2 (k + 1)) x 16 B <= 227 KB with one
-  // CTA per sector
-  int k = 256;
-  while (td_smem_bytes(k + 256, 1) <= 227 * 1024) k += 256;
-  return std::min(k, 32 * 32);   // the back-transformation keeps 32 entries per lane
+  // every k up to the bound fits the tridiagonalisation's shared memory with one CTA per
+  // sector (the row ring shrinks in steps as k grows, so the size is not monotone in k)
+  static const int kmax = [] {
+    int best = 0;
+    for (int k = 1; k <= 32 * 32; ++k) {   // the back-transformation keeps 32 entries per lane
+      if (td_smem_bytes(k, 1) > 227 * 1024) break;
+      best = k;
+    }
+    return best;
+  }();
+  return kmax;
 }
 
 // Size-class bounds (largest k of classes 0, 1, 2); BSMPO_TD_CLASSES="a,b,c" in the
@@ -600,10 +701,13 @@ int tridiag_class(int k) {
 
 cudaError_t launch_tridiag(const SectorDesc* sd_dev, const int* list_dev, const int* class_count,
                            const int* class_kmax, void* gbuf, double* dbuf, double* ebuf,
-                           void* taubuf, const cudaStream_t* streams) {
+                           void* taubuf, int* err, const cudaStream_t* streams) {
   // once per process: the largest dynamic shared memory any launch may ask for
-  static const cudaError_t attr = cudaFuncSetAttribute(
-      tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)td_smem_bytes(eigen_max_k(), 1));
+  static const cudaError_t attr = [] {
+    size_t most = 0;
+    for (int k = 1; k <= eigen_max_k(); ++k) most = std::max(most, td_smem_bytes(k, 1));
+    return cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most);
+  }();
   if (attr != cudaSuccess) return attr;
   int first = 0;
   for (int c = 0; c < TD_CLASSES; ++c) {
@@ -624,7 +728,7 @@ cudaError_t launch_tridiag(const SectorDesc* sd_dev, const int* list_dev, const 
     cfg.numAttrs = 1;
     cudaError_t e = cudaLaunchKernelEx(&cfg, tridiag_kernel, sd_dev, list_dev + first, class_kmax[c],
                                        reinterpret_cast<cplx*>(gbuf), dbuf, ebuf,
-                                       reinterpret_cast<cplx*>(taubuf));
+                                       reinterpret_cast<cplx*>(taubuf), err);
     if (e != cudaSuccess) return e;
     first += count;
   }

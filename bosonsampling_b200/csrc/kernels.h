@@ -167,11 +167,12 @@ int eigen_max_k();
 // Sectors go in four launches by size class (tridiag_class: 1, 2, 4 or 8 CTAs per
 // sector): list_dev holds the sector indices grouped by class, class_count / class_kmax
 // (host, 4 entries) the number of sectors and their largest k per class.  Class c goes
-// on streams[3 - c] (the caller forks and joins them; streams[0] is its own).
+// on streams[3 - c] (the caller forks and joins them; streams[0] is its own).  err: a
+// device word set to 1 when a bulk-copy wait expired (zeroed by the caller).
 int tridiag_class(int k);
 cudaError_t launch_tridiag(const SectorDesc* sd_dev, const int* list_dev, const int* class_count,
                            const int* class_kmax, void* gbuf, double* dbuf, double* ebuf,
-                           void* taubuf, const cudaStream_t* streams);
+                           void* taubuf, int* err, const cudaStream_t* streams);
 // eigenvalues (lam, descending), singular values sig = sqrt(lam) (0 below the floor), 1/sig
 cudaError_t launch_bisect(const SectorDesc* sd_dev, int n_sectors, int kmax, const double* dbuf,
                           const double* ebuf, double* lam, double* sig, double* invsig,

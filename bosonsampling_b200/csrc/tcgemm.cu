@@ -30,6 +30,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "pipeline.cuh"
 
 namespace {
 
@@ -45,55 +46,11 @@ constexpr int RAW_STAGE = RAW_A_BYTES + RAW_B_BYTES;
 constexpr int OP_BYTES = 128 * 2 * TC_BK * 4;     // 128 rows x 16 TF32 = 8 KB
 constexpr int CV_STAGE = 4 * OP_BYTES;            // A hi, A lo, B hi, B lo
 constexpr int TC_SMEM = TC_RAW * RAW_STAGE + TC_CV * CV_STAGE + 1024 + 1024;
-constexpr long long WAIT_CYCLES = 2000000000ll;   // ~1 s at 1.9 GHz
 
 // instruction descriptor, kind::tf32: D F32 (bits 4-5 = 1), A and B TF32 (bits 7-9 and
 // 10-12 = 2), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
 constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(128 >> 3) << 17) |
                               ((uint32_t)(128 >> 4) << 24);
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-
-// waits for the phase with the given parity; false (and the error word set) after
-// WAIT_CYCLES or when another role already failed
-__device__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-  const uint32_t a = smem_u32(bar);
-  const long long t0 = clock64();
-  for (uint32_t it = 0;; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if ((it & 255) == 255) {
-      if (*(volatile int*)err != 0) return false;
-      if (clock64() - t0 > WAIT_CYCLES) {
-        atomicExch(err, 1);
-        return false;
-      }
-    }
-    __nanosleep(20);
-  }
-}
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
                                             uint64_t* bar) {

@@ -169,6 +169,29 @@ class MPOSimulator:
         self._chk(self.L.bsmpo_run_mesh(self.h, len(modes), _capi.iptr(modes), _capi.dptr(theta),
                                         _capi.dptr(phi)))
 
+    def run_mesh_host(self, modes, theta, phi, state_in, state_out=None):
+        """``run_mesh`` over a host-resident state (``bsmpo_run_mesh_host``): ``state_in``
+        = (Gamma complex128 [n,chi,chi], Lambda float64 [n-1,chi], charge int32
+        [n+1,chi,2]) CPU tensors, page-locked for the copies to overlap the updates;
+        the resulting state goes to ``state_out`` (same shapes, may be ``state_in``;
+        new pinned tensors if None), which is returned.  The device keeps the state."""
+        t = self.torch
+        shapes = [(self.n, self.chi, self.chi), (self.n - 1, self.chi), (self.n + 1, self.chi, 2)]
+        dtypes = [t.complex128, t.float64, t.int32]
+        if state_out is None:
+            state_out = tuple(t.empty(sh, dtype=dt, pin_memory=True) for sh, dt in zip(shapes, dtypes))
+        for x in list(state_in) + list(state_out):
+            assert not x.is_cuda and x.is_contiguous()
+        for x, y, sh, dt in zip(state_in, state_out, shapes, dtypes):
+            assert tuple(x.shape) == sh and tuple(y.shape) == sh and x.dtype == dt and y.dtype == dt
+        modes = np.ascontiguousarray(modes, dtype=np.int32)
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        ptr = [ctypes.c_void_p(x.data_ptr()) for x in list(state_in) + list(state_out)]
+        self._chk(self.L.bsmpo_run_mesh_host(self.h, len(modes), _capi.iptr(modes), _capi.dptr(theta),
+                                             _capi.dptr(phi), *ptr))
+        return state_out
+
     def mesh_truncation(self):
         """Truncation weight of every update of the last ``run_mesh`` call (mesh order)."""
         n = self.L.bsmpo_mesh_truncation(self.h, None, 0)

@@ -182,6 +182,23 @@ int bsmpo_bs_update_tensor(bsmpo_ctx* h, int mode, const void* u);
 int bsmpo_run_mesh(bsmpo_ctx* h, int n_bs, const int* modes, const double* theta,
                    const double* phi);
 
+/* The same mesh over a host-resident state (the reference keeps the state in host
+ * memory and moves each update's blocks to the device and back:
+ * src/beam_splitter_parallel/Rank.py:63-68 and 198-199).  The input state
+ * (gamma_in [n][chi][chi] complex128, lambda_in [n-1][chi], charge_in [n+1][chi][2], the
+ * bsmpo_load_state layout, host memory) is validated, its bonds are copied in, and
+ * each site of Gamma is copied in by the first update touching it, on that update's
+ * stream, and copied to gamma_out by the last one, so one update's transfers overlap
+ * the other updates' compute (both directions need page-locked host memory to run
+ * asynchronously).  lambda_out and charge_out are written at the end.  The outputs may
+ * alias the inputs.  On return the device holds the same state (as after
+ * bsmpo_load_state + bsmpo_run_mesh) and all copies are complete.  On error the
+ * device state is not loaded. */
+int bsmpo_run_mesh_host(bsmpo_ctx* h, int n_bs, const int* modes, const double* theta,
+                        const double* phi, const void* gamma_in, const double* lambda_in,
+                        const int* charge_in, void* gamma_out, double* lambda_out,
+                        int* charge_out);
+
 /* Truncation weight (sum of discarded sigma^2) of every update of the last
  * bsmpo_run_mesh call, in mesh order, into host weights[cap].  Returns the number of
  * updates (>= 0; weights == NULL only queries it) or a negative code
