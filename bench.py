@@ -29,6 +29,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 # many hardware work queues as it has worker streams (process-local; read when CUDA
 # initialises, so set before torch is imported)
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+# load every kernel module at context creation: a module loaded lazily by its first
+# launch inside the timed region would stall the concurrent updates
+os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
@@ -435,6 +438,7 @@ def main():
         sim.set_timing(True)
         launches0 = sim.kernel_launches()
         routes0 = sim.svd_routes()
+        ws0 = sim.workspace_stats()
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
@@ -450,13 +454,16 @@ def main():
         sampler.stop()
         launches = sim.kernel_launches() - launches0
         routes = [a - b for a, b in zip(sim.svd_routes(), routes0)]
+        ws1 = sim.workspace_stats()
         svd_ms, svd_flops, svd_launches = sim.jacobi_timing()
         sim.set_timing(False)
         t = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, "cuda")
         tr, P = sim.observables()
         return {"seconds": t, "launches": launches, "svd_ms": svd_ms, "svd_flops": svd_flops,
                 "svd_launches": svd_launches, "clocks": sampler.summary(), "trace": tr, "P": P,
-                "routes": {"jacobi": routes[0], "gram": routes[1]}}
+                "routes": {"jacobi": routes[0], "gram": routes[1]},
+                "workspace_grows": {"device": ws1[0] - ws0[0], "pinned": ws1[1] - ws0[1],
+                                    "device_bytes": ws1[2], "pinned_bytes": ws1[3]}}
 
     # ---- timed, device-resident: the measured path, then the plain FP64 path on the same
     # layers from the same state (the metric's denominator)
@@ -648,6 +655,7 @@ def main():
                                          "stored and copied out one after another"},
             "gpu_launches": int(mine["launches"]),
             "svd_routes": mine["routes"],
+            "workspace_grows_in_timed_region": mine["workspace_grows"],
             "roofline": roofline(args, mine, kernel, fp64_peak, hbm_peak),
             "precision_forms": {form: {
                 "value": r["value"], "unit": "BS-updates/s", "speedup_vs_plain": (r["value"] / plain["value"]) if plain else None,

@@ -49,6 +49,7 @@ SIGNATURES = {
     "bsmpo_bond_dims": (_c_int, [_vp, _ip]),
     "bsmpo_kernel_launches": (ctypes.c_int64, [_vp]),
     "bsmpo_svd_routes": (_c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "bsmpo_workspace_stats": (_c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "bsmpo_stage_times": (_c_int, [_vp, _dp, _c_int]),
     "bsmpo_set_timing": (_c_int, [_vp, _c_int]),
     "bsmpo_jacobi_timing": (_c_int, [_vp, _dp, _dp, ctypes.POINTER(ctypes.c_int64)]),

@@ -57,6 +57,10 @@ struct bsmpo_ctx {
   // workspaces come from this stream-ordered pool (shared with the workers): growing a
   // buffer never synchronises the device, so other workers' streams keep running
   cudaMemPool_t pool = nullptr;
+  // workspace growth: counts, and pinned stages replaced by larger ones (freed at destroy:
+  // releasing pinned memory synchronises the device, which would stall every worker)
+  int64_t dev_grows = 0, host_grows = 0;
+  std::vector<void*> retired_host;
   // host waits of an update sleep on this event (blocking synchronisation) instead of
   // spinning, so several workers' waits leave the host cores to the launching threads
   cudaEvent_t wait_ev = nullptr;
@@ -101,12 +105,13 @@ struct bsmpo_ctx {
   // 1.1e-4 / 1.3e-3 marginal error on the N=16 / N=32 circuits against 8.7e-6 / 1.0e-4
   // with Theta alone)
   int tc_mask = 1;
-  // the tridiagonalisation's four size-class launches go on forked streams (1) or one
-  // after another on the update's stream (0); BSMPO_TD_FORK.  With concurrent updates the
-  // streams of all workers share the device's hardware queues
-  // (CUDA_DEVICE_MAX_CONNECTIONS, at most 32): streams beyond that count are serialised
-  // with others, so the fork pays only while workers x 4 stays within the queues
+  // side streams (0-3, BSMPO_TD_FORK) for the tridiagonalisation's size-class launches:
+  // the largest class present runs on the update's stream, the others on the side
+  // streams, forked and joined with events.  With concurrent updates the streams of all
+  // workers share the device's hardware queues (CUDA_DEVICE_MAX_CONNECTIONS, at most
+  // 32); streams beyond that count are serialised with others
   int td_fork = 1;
+  int n_aux = 0;   // side streams created
   HostStage stage, stage2, hres;
   // last update diagnostics (host)
   std::vector<int> last_cc, last_shape, last_kept, last_k;
@@ -162,12 +167,14 @@ int make_fork_streams(bsmpo_ctx* h) {
     h->fork_ev = nullptr;
     return fail(h, BSMPO_ECUDA, "fork event creation failed");
   }
-  for (int i = 0; i < 3; ++i)
+  for (int i = 0; i < std::min(h->td_fork, 3); ++i) {
     if (cudaStreamCreateWithFlags(&h->aux[i], cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->join_ev[i], cudaEventDisableTiming) != cudaSuccess) {
       cudaGetLastError();
       return fail(h, BSMPO_ECUDA, "fork stream creation failed");
     }
+    h->n_aux = i + 1;
+  }
   return BSMPO_OK;
 }
 
@@ -201,6 +208,7 @@ int grow(bsmpo_ctx* h, DevBuf& b, size_t bytes) {
   b.p = nullptr;
   b.bytes = 0;
   size_t want = align_up(bytes + bytes / 4 + 256, 256);
+  h->dev_grows++;
   if (cudaMallocFromPoolAsync(&b.p, want, h->pool, h->stream) != cudaSuccess) {
     cudaGetLastError();
     b.p = nullptr;
@@ -212,12 +220,13 @@ int grow(bsmpo_ctx* h, DevBuf& b, size_t bytes) {
 
 int grow_host(bsmpo_ctx* h, HostStage& b, size_t bytes) {
   if (bytes <= b.bytes) return BSMPO_OK;
-  CK(h, cudaStreamSynchronize(h->stream));
-  if (b.p) CK(h, cudaFreeHost(b.p));
+  // the old stage may still be read by copies in flight: kept until destroy
+  if (b.p) h->retired_host.push_back(b.p);
   b.p = nullptr;
   b.bytes = 0;
-  // pinned host memory: rare, generous growth (allocation and release are synchronous)
+  // pinned host memory: rare, generous growth
   size_t want = std::max<size_t>(align_up(bytes + bytes / 2 + 256, 256), 1 << 20);
+  h->host_grows++;
   CK(h, cudaMallocHost(&b.p, want));
   b.bytes = want;
   return BSMPO_OK;
@@ -666,9 +675,21 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
     CKL(h, launch_zgemm_grouped(h->abuf.p, h->abuf.p, h->gbuf.p, nullptr, ggram_d, (int)P.ggram.size(),
                                 P.gram_tiles, st));
     {
-      const bool fork = h->td_fork != 0;
-      if (fork && (rc = make_fork_streams(h))) return rc;
-      const cudaStream_t ts[4] = {st, fork ? h->aux[0] : st, fork ? h->aux[1] : st, fork ? h->aux[2] : st};
+      // the largest class present on the update's stream, the others spread over the
+      // side streams (none: all one after another)
+      if (h->td_fork > 0 && (rc = make_fork_streams(h))) return rc;
+      const int naux = std::min(h->td_fork, h->n_aux);
+      cudaStream_t ts[4] = {st, st, st, st};
+      bool used[3] = {false, false, false};
+      for (int c = 3, slot = -1; c >= 0; --c) {
+        if (P.td_count[c] == 0) continue;
+        if (slot >= 0 && naux > 0) {
+          ts[3 - c] = h->aux[slot % naux];
+          used[slot % naux] = true;
+        }
+        ++slot;
+      }
+      const bool fork = used[0] || used[1] || used[2];
       if (h->timing) {
         if (!h->td_ev0) {
           CK(h, cudaEventCreate(&h->td_ev0));
@@ -679,12 +700,12 @@ int bs_update_impl(bsmpo_ctx* h, int mode, const cplx* u3_dev) {
       if (fork) {
         CK(h, cudaEventRecord(h->fork_ev, st));
         for (int i = 0; i < 3; ++i)
-          if (P.td_count[2 - i] > 0) CK(h, cudaStreamWaitEvent(h->aux[i], h->fork_ev, 0));
+          if (used[i]) CK(h, cudaStreamWaitEvent(h->aux[i], h->fork_ev, 0));
       }
       CK(h, launch_tridiag(sd_d, tdlist_d, P.td_count, P.td_kmax, h->gbuf.p, dbuf_d, ebuf_d, h->taub.p,
                            tcerr_d, ts));
-      for (int i = 0; i < 3 && fork; ++i)
-        if (P.td_count[2 - i] > 0) {
+      for (int i = 0; i < 3; ++i)
+        if (used[i]) {
           CK(h, cudaEventRecord(h->join_ev[i], h->aux[i]));
           CK(h, cudaStreamWaitEvent(st, h->join_ev[i], 0));
         }
@@ -1053,6 +1074,8 @@ void free_workspaces(bsmpo_ctx* h) {
   HostStage* hs[] = {&h->stage, &h->stage2, &h->stage3, &h->hres};
   for (HostStage* b : hs)
     if (b->p) cudaFreeHost(b->p);
+  for (void* p : h->retired_host) cudaFreeHost(p);
+  h->retired_host.clear();
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->wait_ev) cudaEventDestroy(h->wait_ev);
@@ -1247,6 +1270,8 @@ int run_mesh_concurrent(bsmpo_ctx* h, int n_bs, const int* modes, const cplx* u3
     h->jac_flops += w->jac_flops;
     h->jac_launches += w->jac_launches;
     h->td_ms += w->td_ms; h->td_bytes += w->td_bytes; h->td_flops += w->td_flops; h->td_phases += w->td_phases;
+    h->dev_grows += w->dev_grows; h->host_grows += w->host_grows;
+    w->dev_grows = w->host_grows = 0;
     w->td_ms = w->td_bytes = w->td_flops = 0.0;
     w->td_phases = 0;
     for (int q = 0; q < 8; ++q) h->stage_ms[q] += w->stage_ms[q];
@@ -1429,7 +1454,7 @@ int bsmpo_create(int n, int d, int chi, int flags, bsmpo_ctx** out) {
   const char* gp = std::getenv("BSMPO_GRAM_POLICY");
   if (gp && gp[0] >= '0' && gp[0] <= '2') h->gram_policy = gp[0] - '0';
   const char* tf = std::getenv("BSMPO_TD_FORK");
-  if (tf && (tf[0] == '0' || tf[0] == '1')) h->td_fork = tf[0] - '0';
+  if (tf && tf[0] >= '0' && tf[0] <= '3') h->td_fork = tf[0] - '0';
   const char* nwk = std::getenv("BSMPO_WORKERS");
   if (nwk && std::atoi(nwk) >= 1 && std::atoi(nwk) <= 64) h->n_workers = std::atoi(nwk);
   *out = h;
@@ -1835,6 +1860,29 @@ int bsmpo_bond_dims(const bsmpo_ctx* h, int* dims) {
 }
 
 int64_t bsmpo_kernel_launches(const bsmpo_ctx* h) { return h ? h->launches : 0; }
+
+int bsmpo_workspace_stats(const bsmpo_ctx* h, int64_t* out) {
+  if (!h || !out) return fail(const_cast<bsmpo_ctx*>(h), BSMPO_EINVAL, "null argument");
+  out[0] = h->dev_grows;
+  out[1] = h->host_grows;
+  // bytes held by the handle and its workers
+  int64_t dev = 0, host = 0;
+  auto add = [&](const bsmpo_ctx* c) {
+    const DevBuf* bufs[] = {&c->theta, &c->cbuf, &c->abuf, &c->wbuf, &c->vbuf, &c->sig, &c->keys,
+                            &c->perm, &c->tab, &c->tab2, &c->rot, &c->kept, &c->u3, &c->m4,
+                            &c->env_l, &c->env_r, &c->part, &c->outv, &c->dims, &c->nf2, &c->qbuf,
+                            &c->qflag, &c->pbuf, &c->pcnt, &c->gbuf, &c->eigd, &c->taub, &c->invsig,
+                            &c->escr, &c->swp, &c->zbuf, &c->ybuf, &c->tab3, &c->tcerr, &c->jwork};
+    for (const DevBuf* b : bufs) dev += (int64_t)b->bytes;
+    const HostStage* hs[] = {&c->stage, &c->stage2, &c->stage3, &c->hres};
+    for (const HostStage* b : hs) host += (int64_t)b->bytes;
+  };
+  add(h);
+  for (const bsmpo_ctx* w : h->workers) add(w);
+  out[2] = dev;
+  out[3] = host;
+  return BSMPO_OK;
+}
 
 int bsmpo_svd_routes(const bsmpo_ctx* h, int64_t* counts) {
   if (!h || !counts) return fail(nullptr, BSMPO_EINVAL, "bad argument");

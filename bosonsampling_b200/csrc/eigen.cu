@@ -50,8 +50,8 @@ constexpr int TD_NT = BSMPO_TD_NT;
 constexpr int TD_CLASSES = 4;   // cluster sizes 1, 2, 4, 8 CTAs per sector, by sector size
 
 constexpr int TD_NW = TD_NT / 32;   // warps per CTA, each streaming its own rows
-// bulk-copy ring of each warp: about BSMPO_TD_RING_KB per CTA, 2 to TD_MAXSLOT row slots
-// (pairs of rows share one pass over the vectors), 1 above k = 768 (shared memory)
+// bulk-copy ring of each warp: about BSMPO_TD_RING_KB per CTA, 1, 2 or TD_MAXSLOT row
+// slots (pairs of rows share one pass over the vectors)
 #ifndef BSMPO_TD_RING_KB
 #define BSMPO_TD_RING_KB 64
 #endif
@@ -59,22 +59,30 @@ constexpr int TD_MAXSLOT = 4;
 #ifndef BSMPO_TD_PAIRS
 #define BSMPO_TD_PAIRS 1   // rows two at a time (0: one at a time)
 #endif
-static_assert(TD_NW >= 1 && TD_NW <= 8, "the per-warp scalars of the tridiagonalisation hold 8 warps");
+static_assert(TD_NW >= 1 && TD_NW <= 8 && (TD_NW & (TD_NW - 1)) == 0,
+              "the tridiagonalisation takes 1, 2, 4 or 8 warps per CTA");
 
-__host__ __device__ inline int td_slots(int kmax) {
-  if (kmax > 768) return 1;
-  const long long s = (long long)BSMPO_TD_RING_KB * 1024 / ((long long)TD_NW * kmax * (long long)sizeof(cplx));
-  return (int)(s < 2 ? 2 : (s > TD_MAXSLOT ? TD_MAXSLOT : s));
-}
-
-// dynamic shared memory of the tridiagonalisation (kmax = largest k of the launch): the
-// row rings, v and w of two steps, the published and the copied row, p of the own rows
-// (two steps), 64 scalars and the rings' mbarriers
-__host__ __device__ inline size_t td_smem_bytes(int kmax, int cl) {
+// shared memory of the tridiagonalisation with `slots` ring slots per warp (kmax = the
+// launch's largest k, cl = CTAs per sector): the row rings, v and w of two steps, the
+// published and the copied row, p of the own rows (two steps), 64 scalars and the rings'
+// mbarriers
+__host__ __device__ inline size_t td_smem_for(int kmax, int cl, int slots) {
   const int own = kmax / cl + 1;
-  return sizeof(cplx) * ((size_t)TD_NW * td_slots(kmax) * kmax + 6 * (size_t)kmax + 2 * (size_t)own) +
+  return sizeof(cplx) * ((size_t)TD_NW * slots * kmax + 6 * (size_t)kmax + 2 * (size_t)own) +
          64 * sizeof(double) + TD_NW * TD_MAXSLOT * sizeof(uint64_t);
 }
+
+// ring slots per warp: a power of two, 2 to TD_MAXSLOT within about BSMPO_TD_RING_KB per
+// CTA, fewer where a one-CTA sector of size kmax would not fit in 227 KB
+__host__ __device__ inline int td_slots(int kmax) {
+  const long long fit = (long long)BSMPO_TD_RING_KB * 1024 / ((long long)TD_NW * kmax * (long long)sizeof(cplx));
+  int s = fit >= TD_MAXSLOT ? TD_MAXSLOT : 2;
+  while (s > 1 && td_smem_for(kmax, 1, s) > 227 * 1024) s >>= 1;
+  return s;
+}
+
+// dynamic shared memory of a tridiagonalisation launch
+__host__ __device__ inline size_t td_smem_bytes(int kmax, int cl) { return td_smem_for(kmax, cl, td_slots(kmax)); }
 
 __device__ __forceinline__ cplx warp_sum(cplx v) {
 #pragma unroll
@@ -146,10 +154,12 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
-  const int TD_CL = (int)cluster.num_blocks();
+  const int TD_CL = (int)cluster.num_blocks();   // 1, 2, 4 or 8
+  const int cls = __ffs(TD_CL) - 1;                // log2 of it
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int own_cap = kmax / TD_CL + 1;
-  const int nslot = td_slots(kmax);
+  const int nslot = td_slots(kmax);                 // 1, 2 or 4
+  const int nss = __ffs(nslot) - 1;
   cplx* ring = reinterpret_cast<cplx*>(smem_raw);  // slot s of warp w: ring + (w nslot + s) kmax
   cplx* vb = ring + (size_t)TD_NW * nslot * kmax;  // v of two consecutive steps: vb + (j & 1) kmax
   cplx* wb = vb + 2 * kmax;                        // w likewise
@@ -180,8 +190,8 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
   // r = warp (mod 4), in step order, then row order; copies are issued in the same order
   // as the pass consumes them, element q into slot q mod nslot
   auto first_row = [&](int s) {
-    const int r0 = s >= rank ? (s - rank) / TD_CL + 1 : 0;
-    return r0 + ((warp - r0) % TD_NW + TD_NW) % TD_NW;
+    const int r0 = s >= rank ? ((s - rank) >> cls) + 1 : 0;
+    return r0 + ((warp - r0) & (TD_NW - 1));
   };
   int is = 0, ir = first_row(0);       // next element to copy
   int issued = 0, done = 0;            // elements copied / consumed
@@ -189,18 +199,18 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
   auto issue = [&]() {
     // a free slot, and the row's write-back of the previous step done (consumption is in
     // sequence order, so the last consumed element tells)
-    while (is < k - 1 && rank + ir * TD_CL < k && issued < done + nslot &&
+    while (is < k - 1 && rank + (ir << cls) < k && issued < done + nslot &&
            (is == 0 || ls > is - 1 || (ls == is - 1 && lr >= ir))) {
       if (lane == 0) {
-        const int slot = issued % nslot;
+        const int slot = issued & (nslot - 1);
         const uint32_t bytes = (uint32_t)(k - is - 1) * (uint32_t)sizeof(cplx);
         mbar_expect_tx(bars + slot, bytes);
-        bulk_load(wring + (size_t)slot * kmax, A + (int64_t)(rank + ir * TD_CL) * k + is + 1, bytes,
+        bulk_load(wring + (size_t)slot * kmax, A + (int64_t)(rank + (ir << cls)) * k + is + 1, bytes,
                   bars + slot);
       }
       ++issued;
       ir += TD_NW;
-      if (rank + ir * TD_CL >= k) ir = first_row(++is);
+      if (rank + (ir << cls) >= k) ir = first_row(++is);
     }
   };
   issue();
@@ -208,7 +218,7 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
   double beta = 0.0;                   // this step's e_j (warp 0)
   for (int j = 0; j < k - 1; ++j) {
     const int par = j & 1;
-    const bool owner = rank == j % TD_CL;
+    const bool owner = rank == (j & (TD_CL - 1));
     cplx* vcur = vb + par * kmax;
     const cplx* vprev = vb + (par ^ 1) * kmax;
     const cplx* wprev = wb + (par ^ 1) * kmax;
@@ -258,14 +268,14 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
       cplx* pw = pown + par * own_cap;
       // rows two at a time where the ring holds two slots: one pass over the vectors for
       // both rows
-      for (int r = first_row(j); rank + r * TD_CL < k;) {
+      for (int r = first_row(j); rank + (r << cls) < k;) {
         const int r2 = r + TD_NW;
-        const int i = rank + r * TD_CL, i2 = rank + r2 * TD_CL;
+        const int i = rank + (r << cls), i2 = rank + (r2 << cls);
         const bool two = BSMPO_TD_PAIRS && nslot >= 2 && i2 < k;   // warp-uniform
-        const int slot = done % nslot, slot2 = (done + 1) % nslot;
+        const int slot = done & (nslot - 1), slot2 = (done + 1) & (nslot - 1);
         // on expiry the error word is set and the pass goes on with what the slot holds
-        mbar_wait(bars + slot, (uint32_t)(done / nslot) & 1u, err);
-        if (two) mbar_wait(bars + slot2, (uint32_t)((done + 1) / nslot) & 1u, err);
+        mbar_wait_fast(bars + slot, (uint32_t)(done >> nss) & 1u, err);
+        if (two) mbar_wait_fast(bars + slot2, (uint32_t)((done + 1) >> nss) & 1u, err);
         const cplx* srow = wring + (size_t)slot * kmax - (j + 1);     // srow[l], l > j
         const cplx* srow2 = wring + (size_t)slot2 * kmax - (j + 1);
         cplx* grow = A + (int64_t)i * k;
@@ -275,40 +285,72 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
         const cplx vi2 = (j > 0 && two) ? vprev[i2] : cmake(0.0, 0.0);
         const cplx wi2 = (j > 0 && two) ? wprev[i2] : cmake(0.0, 0.0);
         cplx acc = cmake(0.0, 0.0), acc2 = cmake(0.0, 0.0);
+        if (two && j > 0 && !next) {
+          // the common case without per-entry tests
 #pragma unroll 2
-        for (int l = j + 1 + lane; l < k; l += 32) {
-          cplx a = ldc(srow + l);
-          cplx a2 = two ? ldc(srow2 + l) : cmake(0.0, 0.0);
-          const cplx vc = ldc(vcur + l);
-          if (j > 0) {
-            const cplx vp = ldc(vprev + l), wp = ldc(wprev + l);
-            a = crank2(a, vi, wp, wi, vp);
+          for (int l = j + 1 + lane; l < k; l += 32) {
+            const cplx vc = ldc(vcur + l), vp = ldc(vprev + l), wp = ldc(wprev + l);
+            const cplx a = crank2(ldc(srow + l), vi, wp, wi, vp);
+            const cplx a2 = crank2(ldc(srow2 + l), vi2, wp, wi2, vp);
             stc(grow + l, a);
-            if (two) {
-              a2 = crank2(a2, vi2, wp, wi2, vp);
-              stc(grow2 + l, a2);
-            }
+            stc(grow2 + l, a2);
+            cfma(acc, a, vc);
+            cfma(acc2, a2, vc);
           }
-          if (next) pub[l] = a;
-          cfma(acc, a, vc);
-          cfma(acc2, a2, vc);
+        } else {
+#pragma unroll 2
+          for (int l = j + 1 + lane; l < k; l += 32) {
+            cplx a = ldc(srow + l);
+            cplx a2 = two ? ldc(srow2 + l) : cmake(0.0, 0.0);
+            const cplx vc = ldc(vcur + l);
+            if (j > 0) {
+              const cplx vp = ldc(vprev + l), wp = ldc(wprev + l);
+              a = crank2(a, vi, wp, wi, vp);
+              stc(grow + l, a);
+              if (two) {
+                a2 = crank2(a2, vi2, wp, wi2, vp);
+                stc(grow2 + l, a2);
+              }
+            }
+            if (next) pub[l] = a;
+            cfma(acc, a, vc);
+            cfma(acc2, a2, vc);
+          }
         }
         // the write-back before the next bulk read of these rows (async proxy)
         if (j > 0) asm volatile("fence.proxy.async.global;" ::: "memory");
-        acc = warp_sum(acc);
-        const cplx p = cmul(tau, acc);
-        if (lane == 0) pw[r] = p;
-        // conj(p_i) v_i, summed by lane 0 of each warp in row order
-        const cplx cv = ccmul(p, vcur[i]);
-        cpx += cv.x;
-        cpy += cv.y;
         if (two) {
-          acc2 = warp_sum(acc2);
-          const cplx p2 = cmul(tau, acc2);
-          if (lane == 0) pw[r2] = p2;
-          const cplx cv2 = ccmul(p2, vcur[i2]);
-          cpx += cv2.x;
-          cpy += cv2.y;
+          // both rows in one butterfly: after the first exchange lanes 0-15 carry row i and
+          // lanes 16-31 row i2; lane 0 ends with row i's sum and fetches row i2's from lane 16
+          const bool hi = (lane & 16) != 0;
+          const cplx send = hi ? acc : acc2;
+          cplx keep = hi ? acc2 : acc;
+          keep.x += __shfl_xor_sync(0xffffffffu, send.x, 16);
+          keep.y += __shfl_xor_sync(0xffffffffu, send.y, 16);
+#pragma unroll
+          for (int o = 8; o > 0; o >>= 1) {
+            keep.x += __shfl_xor_sync(0xffffffffu, keep.x, o);
+            keep.y += __shfl_xor_sync(0xffffffffu, keep.y, o);
+          }
+          acc = keep;
+          acc2 = cmake(__shfl_sync(0xffffffffu, keep.x, 16), __shfl_sync(0xffffffffu, keep.y, 16));
+        } else {
+          acc = warp_sum(acc);
+        }
+        if (lane == 0) {
+          // p_i, and conj(p_i) v_i summed by lane 0 of each warp in row order
+          const cplx p = cmul(tau, acc);
+          pw[r] = p;
+          const cplx cv = ccmul(p, vcur[i]);
+          cpx += cv.x;
+          cpy += cv.y;
+          if (two) {
+            const cplx p2 = cmul(tau, acc2);
+            pw[r2] = p2;
+            const cplx cv2 = ccmul(p2, vcur[i2]);
+            cpx += cv2.x;
+            cpy += cv2.y;
+          }
         }
         __syncwarp();                  // every lane done with the slots and the rows
         done += two ? 2 : 1;
@@ -340,10 +382,10 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
       }
       const cplx a2 = cscale(cmul(tau, cmake(cx, cy)), -0.5);
       cplx* wcur = wb + par * kmax;
-      const cplx* rpub = cluster.map_shared_rank(pub, (j + 1) % TD_CL);
+      const cplx* rpub = cluster.map_shared_rank(pub, (j + 1) & (TD_CL - 1));
       for (int l = j + 1 + tid; l < k; l += TD_NT) {
-        const cplx* rp = cluster.map_shared_rank(pown, l % TD_CL);
-        wcur[l] = cadd(rp[par * own_cap + l / TD_CL], cmul(a2, vcur[l]));
+        const cplx* rp = cluster.map_shared_rank(pown, l & (TD_CL - 1));
+        wcur[l] = cadd(rp[par * own_cap + (l >> cls)], cmul(a2, vcur[l]));
         nrow[l] = rpub[l];
       }
       if (owner) {
@@ -360,7 +402,7 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
     }
   }
   // last diagonal entry: row k - 1 (copied in the last G) minus the update of step k - 2
-  if (rank == (k - 1) % TD_CL && tid == 0) {
+  if (rank == ((k - 1) & (TD_CL - 1)) && tid == 0) {
     const int j = k - 1;
     const cplx v = vb[((k - 2) & 1) * kmax + j], w = wb[((k - 2) & 1) * kmax + j];
     const cplx a = crank2(nrow[j], v, w, w, v);
@@ -688,7 +730,7 @@ int eigen_max_k() {
 // environment replaces them (read once).
 int tridiag_class(int k) {
   static const int* bounds = [] {
-    static int b[3] = {64, 160, 320};
+    static int b[3] = {64, 320, 1024};   // the 8-CTA class stays unused up to k = 1024
     const char* e = std::getenv("BSMPO_TD_CLASSES");
     int x, y, z;
     if (e && std::sscanf(e, "%d,%d,%d", &x, &y, &z) == 3 && 0 < x && x < y && y < z) {

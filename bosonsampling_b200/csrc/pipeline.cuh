@@ -52,6 +52,19 @@ __device__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
   }
 }
 
+// one test of the phase with the given parity, then the bounded wait if it is not done
+__device__ __forceinline__ bool mbar_wait_fast(uint64_t* bar, uint32_t parity, int* err) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done ? true : mbar_wait(bar, parity, err);
+}
+
 // bulk copy global -> this CTA's shared memory (both 16-byte aligned, bytes a multiple of
 // 16), completing `bytes` transactions on `bar`
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {

@@ -262,6 +262,12 @@ class MPOSimulator:
         self._chk(self.L.bsmpo_svd_routes(self.h, c))
         return int(c[0]), int(c[1])
 
+    def workspace_stats(self):
+        """(device allocations, pinned allocations, device bytes held, pinned bytes held)."""
+        c = (ctypes.c_int64 * 4)()
+        self._chk(self.L.bsmpo_workspace_stats(self.h, c))
+        return tuple(int(x) for x in c)
+
     def kernel_launches(self):
         return int(self.L.bsmpo_kernel_launches(self.h))
 

@@ -242,6 +242,14 @@ int bsmpo_bond_dims(const bsmpo_ctx* h, int* dims);
  * creation (host int64[2]). */
 int bsmpo_svd_routes(const bsmpo_ctx* h, int64_t* counts);
 
+/* Workspace growth since creation (host int64[4]): [0] device workspace allocations
+ * (stream-ordered, from the handle's pool), [1] pinned host stage allocations, [2]
+ * device bytes and [3] pinned bytes held now by the handle and its workers.  Workspaces
+ * grow on demand to the largest update seen and are kept until bsmpo_destroy; a
+ * replaced pinned stage is also kept until then (releasing pinned memory would
+ * synchronise the device). */
+int bsmpo_workspace_stats(const bsmpo_ctx* h, int64_t* out);
+
 /* Number of kernels this handle has launched since creation. */
 int64_t bsmpo_kernel_launches(const bsmpo_ctx* h);
 
