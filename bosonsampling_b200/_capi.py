@@ -20,6 +20,7 @@ SIGNATURES = {
     "bsmpo_version": (ctypes.c_char_p, []),
     "bsmpo_last_error": (ctypes.c_char_p, [_vp]),
     "bsmpo_unitary": (_c_int, [_c_int, _dp, _vp, _vp]),
+    "bsmpo_bs_angle_grad": (_c_int, [_c_int, _c_int, _dp, _dp, _vp, _vp, _vp]),
     "bsmpo_unitary_tr": (_c_int, [_c_int, _c_double, _c_double, _c_double, _c_double, _vp, _vp, _vp]),
     "bsmpo_contract_sector": (_c_int, [_c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp,
                                        _c_int, _c_int, _c_int, _vp, _vp]),

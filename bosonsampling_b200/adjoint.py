@@ -1,0 +1,516 @@
+"""Differentiation form: gradients of a loss on the output marginals with respect to every
+beam splitter's (theta, phi) and the input transmissivity eta.
+
+The reference simulates forward only; the update it would differentiate is
+``InitializationMPO.Update`` (``src/MPO.py:234-279``): per new centre charge the block
+product ``C = sum Gamma_L[a, q] w(U) Gamma_R[q, b]``, ``theta = C diag(Lambda_R)``, thin SVD
+``theta = V S Y^H``, keep the top chi over all sectors, ``Gamma_L' = V``, ``Lambda' = S``,
+``Gamma_R' = V^H C``.  The forward here is the library's own update (``bsmpo_bs_update`` /
+``bsmpo_run_mesh`` on the device, plain FP64 path by default).  The backward is a
+hand-derived adjoint of that update, run on the device:
+
+* gauge: ``Gamma_L' Gamma_R' = V V^H C`` and ``Lambda'`` do not depend on the phases of the
+  kept vectors, so the loss is gauge invariant and the adjoint needs no gauge term;
+* SVD: with ``U`` the left vectors (kept ones = the forward's ``V``), ``J = U^H Ubar``,
+  ``theta_bar = U [(F o (J - J^H)) S + diag(Sbar)] Y^H + (I - U U^H) Ubar S^-1 Y^H`` over the
+  whole thin spectrum (the discarded vectors enter through F), with the Lorentzian-
+  broadened ``F_ij = D / (D^2 + eps)``, ``D = s_j^2 - s_i^2`` (``eps = (1e-12 s_max^2)^2``);
+* contraction: ``Gamma_L_bar[:, q] += (Cbar o conj(w_q)) Gamma_R[q, :]^H``,
+  ``Gamma_R_bar[q, :] += Gamma_L[:, q]^H (Cbar o conj(w_q))``, and the gate weights' gradient
+  from the block sums of ``Cbar o conj(Gamma_L[:, q] Gamma_R[q, :])``, turned into
+  dL/dtheta, dL/dphi on the device (``bsmpo_bs_angle_grad``);
+* memory: the MPO is checkpointed every ``checkpoint_layers`` mesh layers; each segment is
+  recomputed update by update on the backward pass.
+
+The loss, the output phases and the marginals are plain torch operations on the device
+(autograd glue); the initial product state's dependence on eta is the derivative of
+its entries (1 - eta, eta).
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _capi, engine
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class StateT:
+    """A device state (Gamma [n, chi, chi], Lambda [n-1, chi]) with host charges."""
+
+    def __init__(self, G, Lam, charge, d):
+        self.G, self.Lam, self.d = G, Lam, d
+        self.charge = charge if isinstance(charge, np.ndarray) else charge.cpu().numpy()
+        self.n, self.chi = int(G.shape[0]), int(G.shape[1])
+        self._lam_host = None
+
+    def lam_host(self, b):
+        if b == 0 or b == self.n:
+            return np.ones(self.chi)
+        if self._lam_host is None:
+            self._lam_host = self.Lam.cpu().numpy()
+        return self._lam_host[b - 1]
+
+    def lam_dev(self, b):
+        torch = _torch()
+        if b == 0 or b == self.n:
+            return torch.ones(self.chi, dtype=torch.float64, device=self.G.device)
+        return self.Lam[b - 1]
+
+    def valid(self, b):
+        return (self.charge[b, :, 0] < self.d) & (self.lam_host(b) > 0)
+
+
+def state_of(sim):
+    g, lam, c = sim.store()
+    return StateT(g, lam, c, sim.d)
+
+
+_GRIDS = {}
+
+
+def _block_grid(d):
+    """Charge grids (a0, a1, q0, q1, b0, b1), each of shape (d,)*6."""
+    if d not in _GRIDS:
+        _GRIDS[d] = np.meshgrid(*([np.arange(d)] * 6), indexing="ij")
+    return _GRIDS[d]
+
+
+def _block_weights(U3h, d, cc0, cc1):
+    """Gate weight w[a, q, b] (a, q, b = charge blocks c0 * d + c1) of sector (cc0, cc1):
+    U3[a0-cc0, cc0-b0, a0-q0] conj(U3[a1-cc1, cc1-b1, a1-q1]) where b <= q <= a and the
+    rows / columns belong to the sector, else 0; with the flat U3 indices of both factors."""
+    A0, A1, Q0, Q1, B0, B1 = _block_grid(d)
+    ok = ((A0 >= cc0) & (A1 >= cc1) & (B0 <= cc0) & (B1 <= cc1) &
+          (B0 <= Q0) & (Q0 <= A0) & (B1 <= Q1) & (Q1 <= A1))
+    i0 = np.where(ok, ((A0 - cc0) * d + (cc0 - B0)) * d + (A0 - Q0), 0)
+    i1 = np.where(ok, ((A1 - cc1) * d + (cc1 - B1)) * d + (A1 - Q1), 0)
+    u = U3h.reshape(-1)
+    w = np.where(ok, u[i0] * np.conj(u[i1]), 0.0)
+    sh = (d * d, d * d, d * d)
+    # axes (a0, a1, q0, q1, b0, b1) -> [a, q, b]
+    return w.reshape(sh), ok.reshape(sh), i0.reshape(sh), i1.reshape(sh)
+
+
+def sector_range(st, m):
+    """Range of new centre charges of the update at mode m (as the forward's)."""
+    d = st.d
+    CL, CR = st.charge[m], st.charge[m + 2]
+    vl, vr = st.valid(m), st.valid(m + 2)
+    hi0 = int(CL[vl, 0].max()) if vl.any() else 0
+    hi1 = int(CL[vl, 1].max()) if vl.any() else 0
+    lo0 = int(CR[vr, 0].min()) if vr.any() else 0
+    lo1 = int(CR[vr, 1].min()) if vr.any() else 0
+    return lo0, hi0, lo1, hi1
+
+
+def svd_backward(theta, V, Vbar, Sbar, eps_rel=1e-12):
+    """Adjoint of the truncated thin SVD: gradient of theta (m x n) given the gradients of
+    the kept left vectors (Vbar, m x k; V = the forward's kept vectors) and of the kept
+    singular values (Sbar, k).  Uses the whole thin spectrum of theta, so the discarded
+    singular values enter the kept vectors' terms."""
+    torch = _torch()
+    m, k = V.shape
+    if theta.is_cuda:
+        U, S, Yh = torch.linalg.svd(theta, full_matrices=False, driver="gesvd")
+    else:
+        U, S, Yh = torch.linalg.svd(theta, full_matrices=False)
+    r = S.shape[0]
+    Y = Yh.conj().transpose(0, 1).contiguous()
+    U = U.contiguous()
+    if k:
+        # the forward's gauge on the kept columns (u_i -> u_i ph_i, y_i -> y_i ph_i)
+        ph = (U[:, :k].conj() * V).sum(0)
+        ph = ph / ph.abs().clamp_min(1e-300)
+        U[:, :k] = V
+        Y[:, :k] = Y[:, :k] * ph[None, :]
+    Ub = torch.zeros((m, r), dtype=theta.dtype, device=theta.device)
+    Ub[:, :k] = Vbar
+    J = U.conj().transpose(0, 1) @ Ub
+    s2 = S * S
+    D = s2[None, :] - s2[:, None]                   # s_j^2 - s_i^2
+    eps = (eps_rel * float(s2.max())) ** 2 if r else 0.0
+    F = D / (D * D + eps)
+    F.fill_diagonal_(0.0)
+    core = (F * (J - J.conj().transpose(0, 1))) * S[None, :].to(theta.dtype)
+    core = core + torch.diag(torch.cat([Sbar, Sbar.new_zeros(r - k)]).to(theta.dtype))
+    g = U @ core @ Y.conj().transpose(0, 1)
+    if m > r and k:
+        P = Vbar - U @ (U.conj().transpose(0, 1) @ Vbar)
+        g = g + (P / S[:k][None, :].to(theta.dtype)) @ Y[:, :k].conj().transpose(0, 1)
+    return g
+
+
+def _qblocks(st, m):
+    """Centre charge blocks (q0, q1, device index tensor) of the update at mode m."""
+    torch = _torch()
+    d, CC, vC = st.d, st.charge[m + 1], st.valid(m + 1)
+    out = []
+    for q0 in range(d):
+        for q1 in range(d):
+            idx = np.nonzero(vC & (CC[:, 0] == q0) & (CC[:, 1] == q1))[0]
+            if len(idx):
+                out.append((q0, q1, torch.as_tensor(idx, device=st.G.device)))
+    return out
+
+
+def update_backward(before, after, m, U3, Gbar, Lbar):
+    """Backward of one update at mode m from ``before`` to ``after`` (StateT) with gate
+    tensor U3 (device complex128 [d, d, d]).  Gbar [n, chi, chi] and Lbar [n-1, chi]
+    (device) hold the gradients with respect to the state after the update; on return
+    they hold those with respect to the state before it.  Returns the gradient of the
+    gate tensor (device complex128 [d, d, d])."""
+    torch = _torch()
+    d, chi, n = before.d, before.chi, before.n
+    dev, ct = before.G.device, before.G.dtype
+    GL, GR = before.G[m], before.G[m + 1]
+    lamR = before.lam_dev(m + 2)
+    CL, CR = before.charge[m], before.charge[m + 2]
+    vL, vR = before.valid(m), before.valid(m + 2)
+    qb = _qblocks(before, m)
+    X = [GL[:, idx] @ GR[idx, :] for (_, _, idx) in qb]
+    # outputs of the forward and the incoming gradients
+    GLp, GRp = after.G[m], after.G[m + 1]
+    CCp, vCp = after.charge[m + 1], after.valid(m + 1)
+    GbL, GbR = Gbar[m].clone(), Gbar[m + 1].clone()
+    Sb_all = Lbar[m].clone() if 0 < m + 1 < n else None
+    gGL = torch.zeros((chi, chi), dtype=ct, device=dev)
+    gGR = torch.zeros((chi, chi), dtype=ct, device=dev)
+    gLR = torch.zeros(chi, dtype=torch.float64, device=dev)
+    U3h = U3.cpu().numpy()
+    u_flat = U3h.reshape(-1)
+    ubar = np.zeros(d ** 3, dtype=np.complex128)
+    wbar_dev, wbar_meta = [], []      # block sums of the weights' gradient, read once at the end
+    lo0, hi0, lo1, hi1 = sector_range(before, m)
+    for cc0 in range(lo0, hi0 + 1):
+        for cc1 in range(lo1, hi1 + 1):
+            l_idx = np.nonzero(vL & (CL[:, 0] >= cc0) & (CL[:, 1] >= cc1))[0]
+            r_idx = np.nonzero(vR & (CR[:, 0] <= cc0) & (CR[:, 1] <= cc1))[0]
+            if not len(l_idx) or not len(r_idx):
+                continue
+            slots = np.nonzero(vCp & (CCp[:, 0] == cc0) & (CCp[:, 1] == cc1))[0]
+            if not len(slots):
+                continue                    # truncated away: no path to the loss
+            li = torch.as_tensor(l_idx, device=dev)
+            ri = torch.as_tensor(r_idx, device=dev)
+            sl = torch.as_tensor(slots, device=dev)
+            wb, ok, i0, i1 = _block_weights(U3h, d, cc0, cc1)
+            ablk = torch.as_tensor((CL[l_idx, 0] * d + CL[l_idx, 1]).astype(np.int64), device=dev)
+            bblk = torch.as_tensor((CR[r_idx, 0] * d + CR[r_idx, 1]).astype(np.int64), device=dev)
+            wb_dev = torch.as_tensor(wb, device=dev)
+            # forward recompute of the sector
+            ws, C = [], torch.zeros((len(l_idx), len(r_idx)), dtype=ct, device=dev)
+            for t, (q0, q1, cidx) in enumerate(qb):
+                q = q0 * d + q1
+                if not ok[:, q, :].any():
+                    ws.append(None)
+                    continue
+                w = wb_dev[:, q, :][ablk][:, bblk]
+                ws.append(w)
+                C = C + X[t][li][:, ri] * w
+            theta = C * lamR[ri][None, :]
+            # gradients of the outputs: Gamma_L' = V, Gamma_R' = V^H C, Lambda' = S
+            V = GLp[li][:, sl]
+            Wb = GbR[sl][:, ri]
+            Vb = GbL[li][:, sl] + C @ Wb.conj().transpose(0, 1)
+            Sb = Sb_all[sl] if Sb_all is not None else torch.zeros(len(slots), dtype=torch.float64, device=dev)
+            Cb = V @ Wb
+            tb = svd_backward(theta, V, Vb, Sb)
+            Cb = Cb + tb * lamR[ri][None, :]
+            gLR.index_add_(0, ri, (tb.conj() * C).real.sum(0))
+            # contraction adjoint
+            Ra = torch.nn.functional.one_hot(ablk, d * d).to(ct)
+            Rb = torch.nn.functional.one_hot(bblk, d * d).to(ct)
+            for t, (q0, q1, cidx) in enumerate(qb):
+                w = ws[t]
+                if w is None:
+                    continue
+                q = q0 * d + q1
+                Cw = Cb * w.conj()
+                gGL.index_put_((li[:, None], cidx[None, :]), Cw @ GR[cidx][:, ri].conj().transpose(0, 1),
+                               accumulate=True)
+                gGR.index_put_((cidx[:, None], ri[None, :]), GL[li][:, cidx].conj().transpose(0, 1) @ Cw,
+                               accumulate=True)
+                # gradient of the block weights: block sums of Cbar o conj(X_q)
+                wbar_dev.append(Ra.transpose(0, 1) @ (Cb * X[t][li][:, ri].conj()) @ Rb)
+                wbar_meta.append((ok[:, q, :], i0[:, q, :], i1[:, q, :]))
+    if wbar_dev:
+        allw = torch.stack(wbar_dev).cpu().numpy()
+        for wbar, (okq, i0q, i1q) in zip(allw, wbar_meta):
+            u0, u1 = u_flat[i0q], u_flat[i1q]
+            np.add.at(ubar, i0q[okq], (wbar * u1)[okq])
+            np.add.at(ubar, i1q[okq], (np.conj(wbar) * u0)[okq])
+    Gbar[m] = gGL
+    Gbar[m + 1] = gGR
+    if 0 < m + 1 < n:
+        Lbar[m].zero_()                     # the old centre Lambda only masks
+    if m + 2 < n:
+        Lbar[m + 1] += gLR
+    return torch.as_tensor(ubar.reshape(d, d, d), device=dev)
+
+
+# ----------------------------------------------------------------------------- observables
+def _diag_masks(charge, lam_host_fn, n, d):
+    return [(charge[b, :, 0] == charge[b, :, 1]) & (charge[b, :, 0] < d) & (lam_host_fn(b) > 0)
+            for b in range(n + 1)]
+
+
+def marginals_torch(G, charge, lam_host_fn, d):
+    """(trace, P[n, d]) of the MPO Gamma_0 ... Gamma_{n-1} as differentiable torch
+    operations (the same environments as the library's observables)."""
+    torch = _torch()
+    n = G.shape[0]
+    dev, ct = G.device, G.dtype
+    masks = [torch.as_tensor(mk, device=dev).to(ct) for mk in _diag_masks(charge, lam_host_fn, n, d)]
+    R = [None] * (n + 1)
+    R[n] = masks[n]
+    for b in range(n - 1, -1, -1):
+        R[b] = masks[b] * (G[b] @ R[b + 1])
+    L = [None] * (n + 1)
+    L[0] = masks[0]
+    for b in range(n):
+        L[b + 1] = masks[b + 1] * (L[b] @ G[b])
+    P = []
+    for i in range(n):
+        occ = (charge[i, :, 0].astype(np.int64)[:, None] - charge[i + 1, :, 0].astype(np.int64)[None, :])
+        M = L[i][:, None] * G[i] * R[i + 1][None, :]
+        row = []
+        for k in range(d):
+            sel = torch.as_tensor(occ == k, device=dev)
+            row.append((M * sel).sum())
+        P.append(torch.stack(row))
+    return R[0].sum(), torch.stack(P)
+
+
+def phase_factors(charge, phases, d, device):
+    """Factors e^{i phi_m (dk - db)} of the output phase screen, per site [n, chi, chi]."""
+    torch = _torch()
+    n = charge.shape[0] - 1
+    a = charge[:-1].astype(np.int64)
+    b = charge[1:].astype(np.int64)
+    dk = a[:, :, None, 0] - b[:, None, :, 0]
+    db = a[:, :, None, 1] - b[:, None, :, 1]
+    valid = (a[:, :, None, 0] < d) & (b[:, None, :, 0] < d)
+    ph = np.asarray(phases, dtype=np.float64)[:, None, None]
+    f = np.where(valid, np.exp(1j * ph * (dk - db)), 1.0)
+    return torch.as_tensor(f, device=device)
+
+
+def marginal_loss(P, tr, target):
+    """Squared L2 distance between the normalised marginals and ``target`` [n, d]."""
+    return ((P.real / tr.real - target) ** 2).sum()
+
+
+# ----------------------------------------------------------------------------- gates
+def gate_tensor(d, theta, phi, device):
+    """The mesh beam splitter's tensor U[new_a][new_b][old_a] of T(theta, phi) (as
+    bsmpo_run_mesh builds it), complex128 [d, d, d] on the device."""
+    torch = _torch()
+    L = _capi.lib()
+    c, s = math.cos(theta), math.sin(theta)
+    e = complex(math.cos(phi), math.sin(phi))
+    # M = T^T, T = [[e c, -s], [e s, c]]; 8 doubles (re, im of M00, M01, M10, M11)
+    M = np.array([(e * c).real, (e * c).imag, (e * s).real, (e * s).imag, -s, 0.0, c, 0.0])
+    u = torch.empty((d, d, d), dtype=torch.complex128, device=device)
+    _capi.check(L.bsmpo_unitary(d, _capi.dptr(M), ctypes.c_void_p(u.data_ptr()),
+                                ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), None)
+    return u
+
+
+def identity_tensor(d, device):
+    """The tensor of the identity gate (the canonicalising sweep's)."""
+    return gate_tensor(d, 0.0, 0.0, device)
+
+
+def angle_grads(d, thetas, phis, ubar):
+    """(dL/dtheta, dL/dphi) of every gate from its tensor gradients ubar [n_gates, d, d, d]."""
+    torch = _torch()
+    L = _capi.lib()
+    ng = len(thetas)
+    th = np.ascontiguousarray(thetas, dtype=np.float64)
+    ph = np.ascontiguousarray(phis, dtype=np.float64)
+    ub = ubar.to(torch.complex128).contiguous()
+    out = torch.zeros((ng, 2), dtype=torch.float64, device=ub.device)
+    _capi.check(L.bsmpo_bs_angle_grad(d, ng, _capi.dptr(th), _capi.dptr(ph), ctypes.c_void_p(ub.data_ptr()),
+                                      ctypes.c_void_p(out.data_ptr()),
+                                      ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), None)
+    return out[:, 0], out[:, 1]
+
+
+# ----------------------------------------------------------------------------- circuits
+def _t_matrix(theta, phi):
+    c, s = math.cos(theta), math.sin(theta)
+    e = complex(math.cos(phi), math.sin(phi))
+    return np.array([[e * c, -s], [e * s, c]], dtype=np.complex128)
+
+
+class DiffCircuit:
+    """A lossy-single-photon circuit whose output marginals are differentiable in every
+    beam splitter's (theta, phi) and in eta.
+
+    ``mesh``: (layer, mode, theta, phi) in circuit order (``interferometer.circuit``);
+    ``phases``: the output phase screen (it leaves the marginals unchanged but is part of
+    the forward).  The forward runs on the library (``precision``, default the plain FP64
+    path); ``checkpoint_layers`` mesh layers lie between two stored states."""
+
+    def __init__(self, n, d, chi, photon_modes, mesh, phases, precision="fp64", workers=8,
+                 checkpoint_layers=4):
+        self.n, self.d, self.chi = n, d, chi
+        self.photon_modes = list(photon_modes)
+        self.mesh = [(int(l), int(m)) for (l, m, _, _) in mesh]
+        self.phases = np.asarray(phases, dtype=np.float64)
+        self.k = int(checkpoint_layers)
+        self.sim = engine.MPOSimulator(n, d, chi)
+        self.sim.set_precision(precision)
+        self.sim.set_workers(workers)
+        nl = max([l for (l, _) in self.mesh] + [-1]) + 1
+        self.layers = [[i for i, (l, _) in enumerate(self.mesh) if l == L] for L in range(nl)]
+
+    def close(self):
+        self.sim.close()
+
+    # the forward, on the library only (no records)
+    def run(self, thetas, phis, eta):
+        """(trace, P) of the circuit with these angles, from the library's observables."""
+        sim = self.sim
+        sim.init_single_photons(self.photon_modes, eta)
+        for L in self.layers:
+            if L:
+                sim.run_mesh([self.mesh[i][1] for i in L], [thetas[i] for i in L], [phis[i] for i in L])
+        sim.apply_phases(self.phases)
+        return sim.observables()
+
+    def _load(self, st):
+        self.sim.load(st.G, st.Lam, st.charge_dev)
+
+    def _state(self):
+        g, lam, c = self.sim.store()
+        st = StateT(g, lam, c, self.d)
+        st.charge_dev = c
+        return st
+
+    def forward_records(self, thetas, phis, eta):
+        """Runs the circuit keeping the product state, the checkpoints and the final state."""
+        sim = self.sim
+        sim.init_single_photons(self.photon_modes, eta, canonicalize=False)
+        prod = self._state()
+        sim.canonicalize()
+        ckpts = []
+        for L0 in range(0, len(self.layers), self.k):
+            ckpts.append(self._state())
+            for L in self.layers[L0:L0 + self.k]:
+                if L:
+                    sim.run_mesh([self.mesh[i][1] for i in L], [thetas[i] for i in L], [phis[i] for i in L])
+        return prod, ckpts, self._state()
+
+    def backward(self, thetas, phis, eta, prod, ckpts, final, Gbar):
+        """Gradients (theta [n_bs], phi [n_bs], eta) from Gbar = dL/dGamma of the final
+        state (before the phase screen)."""
+        torch = _torch()
+        d, n, chi = self.d, self.n, self.chi
+        dev = final.G.device
+        Gbar = Gbar.clone()
+        Lbar = torch.zeros((n - 1, chi), dtype=torch.float64, device=dev)
+        ubar = torch.zeros((len(self.mesh), d, d, d), dtype=torch.complex128, device=dev)
+        for j in range(len(ckpts) - 1, -1, -1):
+            ops = [i for L in self.layers[j * self.k:(j + 1) * self.k] for i in L]
+            self._load(ckpts[j])
+            recs = [ckpts[j]]
+            gates = []
+            for i in ops:
+                m = self.mesh[i][1]
+                self.sim.bs_update(m, _t_matrix(thetas[i], phis[i]))
+                recs.append(self._state())
+                gates.append(gate_tensor(d, thetas[i], phis[i], dev))
+            for t in range(len(ops) - 1, -1, -1):
+                i = ops[t]
+                ubar[i] = update_backward(recs[t], recs[t + 1], self.mesh[i][1], gates[t], Gbar, Lbar)
+            del recs
+        # the canonicalising sweep (identity gates, right to left)
+        self._load(prod)
+        recs = [prod]
+        ident = identity_tensor(d, dev)
+        sweep = list(range(n - 2, -1, -1))
+        for m in sweep:
+            self.sim.bs_update(m, np.eye(2, dtype=np.complex128))
+            recs.append(self._state())
+        for t in range(len(sweep) - 1, -1, -1):
+            update_backward(recs[t], recs[t + 1], sweep[t], ident, Gbar, Lbar)
+        del recs
+        # eta: the product state's entries are (1 - eta) at occupation (0, 0) and eta at
+        # (1, 1) on the photon modes
+        g_eta = 0.0
+        for i in self.photon_modes:
+            a = prod.charge[i].astype(np.int64)
+            b = prod.charge[i + 1].astype(np.int64)
+            ok = (a[:, None, 0] < d) & (b[None, :, 0] < d)
+            o0 = a[:, None, 0] - b[None, :, 0]
+            o1 = a[:, None, 1] - b[None, :, 1]
+            dG = np.where(ok & (o0 == 0) & (o1 == 0), -1.0, 0.0) + np.where(ok & (o0 == 1) & (o1 == 1), 1.0, 0.0)
+            g_eta += float((Gbar[i].real * torch.as_tensor(dG, device=dev)).sum())
+        g_th, g_ph = angle_grads(d, thetas, phis, ubar)
+        return g_th, g_ph, g_eta
+
+    def loss_and_grad(self, thetas, phis, eta, target):
+        """(loss, dL/dtheta, dL/dphi, dL/deta) of the marginal loss against ``target``."""
+        torch = _torch()
+        prod, ckpts, final = self.forward_records(thetas, phis, eta)
+        G = final.G.clone().requires_grad_(True)
+        f = phase_factors(final.charge, self.phases, self.d, G.device)
+        tr, P = marginals_torch(G * f, final.charge, final.lam_host, self.d)
+        tgt = torch.as_tensor(np.asarray(target, dtype=np.float64), device=G.device)
+        loss = marginal_loss(P, tr, tgt)
+        loss.backward()
+        g_th, g_ph, g_eta = self.backward(thetas, phis, eta, prod, ckpts, final, G.grad)
+        return float(loss.detach()), g_th, g_ph, g_eta
+
+
+class CircuitMarginals:
+    """``torch.autograd.Function`` form: ``CircuitMarginals.apply(thetas, phis, eta,
+    circuit)`` returns (trace, P [n, d]) of a :class:`DiffCircuit`; any loss built on them
+    backpropagates through the adjoint into the three parameter tensors."""
+
+    @staticmethod
+    def apply(thetas, phis, eta, circuit):
+        return _marginals_function().apply(thetas, phis, eta, circuit)
+
+
+_FN = None
+
+
+def _marginals_function():
+    global _FN
+    if _FN is None:
+        torch = _torch()
+
+        class _Fn(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, thetas, phis, eta, circuit):
+                th = thetas.detach().cpu().numpy().astype(np.float64)
+                ph = phis.detach().cpu().numpy().astype(np.float64)
+                e = float(eta.detach())
+                prod, ckpts, final = circuit.forward_records(th, ph, e)
+                ctx.saved = (circuit, th, ph, e, prod, ckpts, final)
+                f = phase_factors(final.charge, circuit.phases, circuit.d, final.G.device)
+                with torch.no_grad():
+                    tr, P = marginals_torch(final.G * f, final.charge, final.lam_host, circuit.d)
+                return tr, P
+
+            @staticmethod
+            def backward(ctx, g_tr, g_P):
+                circuit, th, ph, e, prod, ckpts, final = ctx.saved
+                with torch.enable_grad():
+                    G = final.G.clone().requires_grad_(True)
+                    f = phase_factors(final.charge, circuit.phases, circuit.d, G.device)
+                    tr, P = marginals_torch(G * f, final.charge, final.lam_host, circuit.d)
+                    torch.autograd.backward([tr, P], [g_tr, g_P])
+                g_th, g_ph, g_eta = circuit.backward(th, ph, e, prod, ckpts, final, G.grad)
+                dev = g_P.device
+                return (g_th.to(dev), g_ph.to(dev), torch.tensor(g_eta, dtype=torch.float64, device=dev), None)
+
+        _FN = _Fn
+    return _FN

@@ -1328,6 +1328,41 @@ const char* bsmpo_last_error(const bsmpo_ctx* h) {
   return g_last_error.c_str();
 }
 
+int bsmpo_bs_angle_grad(int d, int n_gates, const double* theta, const double* phi, const void* ubar,
+                        double* grad, void* stream) {
+  if (d < 1 || d > BSMPO_MAX_D || n_gates < 0 || (n_gates > 0 && (!theta || !phi || !ubar || !grad)))
+    return fail(nullptr, BSMPO_EINVAL, "bad argument");
+  if (n_gates == 0) return BSMPO_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  // per gate: M = T^T and dM/dtheta, dM/dphi of T(theta, phi) = [[e^{i phi} c, -s], [e^{i phi} s, c]]
+  std::vector<double> m4((size_t)n_gates * 8), dm4((size_t)n_gates * 16);
+  for (int g = 0; g < n_gates; ++g) {
+    const double c = std::cos(theta[g]), s = std::sin(theta[g]);
+    const double er = std::cos(phi[g]), ei = std::sin(phi[g]);
+    const double T[8] = {er * c, ei * c, -s, 0.0, er * s, ei * s, c, 0.0};
+    const double Tt[8] = {-er * s, -ei * s, -c, 0.0, er * c, ei * c, -s, 0.0};        // dT/dtheta
+    const double Tp[8] = {-ei * c, er * c, 0.0, 0.0, -ei * s, er * s, 0.0, 0.0};      // dT/dphi
+    const M8 a = transpose_to_m8(T), b = transpose_to_m8(Tt), e = transpose_to_m8(Tp);
+    for (int j = 0; j < 8; ++j) {
+      m4[(size_t)g * 8 + j] = a.v[j];
+      dm4[(size_t)g * 16 + j] = b.v[j];
+      dm4[(size_t)g * 16 + 8 + j] = e.v[j];
+    }
+  }
+  void* dev = nullptr;
+  const size_t bytes = (m4.size() + dm4.size()) * sizeof(double);
+  cudaError_t e = cudaMallocAsync(&dev, bytes, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dev, m4.data(), m4.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+  double* dm4_dev = static_cast<double*>(dev) + m4.size();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dm4_dev, dm4.data(), dm4.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = launch_fock_angle_grad(d, n_gates, static_cast<double*>(dev), dm4_dev, ubar, grad, st);
+  if (dev) cudaFreeAsync(dev, st);
+  const cudaError_t e2 = cudaStreamSynchronize(st);   // the host arrays above are read by the copies
+  if (e == cudaSuccess) e = e2;
+  if (e != cudaSuccess) return fail(nullptr, BSMPO_ECUDA, cudaGetErrorString(e));
+  return BSMPO_OK;
+}
+
 int bsmpo_unitary(int d, const double* M, void* u_out, void* stream) {
   if (d < 1 || d > BSMPO_MAX_D || !M || !u_out) return fail(nullptr, BSMPO_EINVAL, "bad argument");
   M8 m;

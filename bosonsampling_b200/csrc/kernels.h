@@ -19,6 +19,11 @@ cudaError_t launch_fock_tensor(int d, int n_gates, const double* m4_dev, void* u
 // One gate with M passed by value; writes interleaved complex (u_im == nullptr) or
 // split real / imaginary double arrays.
 struct M8 { double v[8]; };
+// dL/dtheta, dL/dphi of every gate T(theta, phi) from the gradient of its tensor: m4 and
+// dm4 (device) hold per gate M (8 doubles) and dM/dtheta, dM/dphi (16 doubles); grad gets
+// 2 doubles per gate.
+cudaError_t launch_fock_angle_grad(int d, int n_gates, const double* m4_dev, const double* dm4_dev,
+                                   const void* ubar_dev, double* grad_dev, cudaStream_t s);
 cudaError_t launch_fock_tensor_single(int d, M8 m, void* u_re_or_cplx, double* u_im,
                                       cudaStream_t s);
 

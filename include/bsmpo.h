@@ -44,6 +44,16 @@ const char* bsmpo_version(void);
 /* Message of the last error on `h` (or of the last handle-less call when h == NULL). */
 const char* bsmpo_last_error(const bsmpo_ctx* h);
 
+/* Gradient with respect to the angles of n_gates mesh beam splitters T(theta, phi) =
+ * [[e^{i phi} cos, -sin], [e^{i phi} sin, cos]] (host theta[], phi[]), given ubar
+ * (device complex128 [n_gates][d][d][d]), the gradient of a real loss with respect to each
+ * gate's tensor U[new_a][new_b][old_a] (as bsmpo_run_mesh builds it; pairing
+ * Re sum conj(ubar) dU).  Writes grad (device double [n_gates][2]: dL/dtheta, dL/dphi).
+ * The reference has no gradient (it runs forward only); the differentiation form's
+ * adjoint (bosonsampling_b200.adjoint) uses this for the gates.  Synchronises stream. */
+int bsmpo_bs_angle_grad(int d, int n_gates, const double* theta, const double* phi,
+                        const void* ubar, double* grad, void* stream);
+
 /* Two-mode Fock beam-splitter tensor.  Replaces cuda_kernels.Rand_U / u_kernel
  * (src/cuda_kernels.py:18-50, src/u_kernel.cu:37-71) and the CPU Rand_BS_MPS
  * (src/MPO.py:6-18).  M is the 2x2 single-particle matrix of the reference's
