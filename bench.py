@@ -659,11 +659,15 @@ def main():
                 fd = ((gloss(vp, gphi, geta) - gloss(vm, gphi, geta)) if kind == "theta"
                       else (gloss(gth, vp, geta) - gloss(gth, vm, geta))) / (2 * h)
                 g = float(g_th[i] if kind == "theta" else g_ph[i])
-            err = abs(g - fd) / max(abs(fd), 1e-12)
-            errs.append(err)
+            errs.append((g, fd))
             checks.append({"param": kind if kind == "eta" else "%s[%d]" % (kind, i), "adjoint": g,
-                           "finite_difference": fd, "rel_err": err})
+                           "finite_difference": fd})
         circ.close()
+        # relative to each finite difference, floored at 1e-3 of the largest one checked
+        scale = max(abs(fd) for _, fd in errs)
+        for c, (g, fd) in zip(checks, errs):
+            c["rel_err"] = abs(g - fd) / max(abs(fd), 1e-3 * scale)
+        errs = [c["rel_err"] for c in checks]
         grad = {"config": "N=24, 12 photons (even modes), eta=0.5, d=4, chi=256, Haar seed %d -> %d-BS mesh; "
                           "target: marginals of Haar seed %d" % (gseed, nb, gseed + 1),
                 "loss": gl, "params": 2 * nb + 1, "forward_seconds": round(t_fwd, 3),

@@ -14,7 +14,12 @@ hand-derived adjoint of that update, run on the device:
 * SVD: with ``U`` the left vectors (kept ones = the forward's ``V``), ``J = U^H Ubar``,
   ``theta_bar = U [(F o (J - J^H)) S + diag(Sbar)] Y^H + (I - U U^H) Ubar S^-1 Y^H`` over the
   whole thin spectrum (the discarded vectors enter through F), with the Lorentzian-
-  broadened ``F_ij = D / (D^2 + eps)``, ``D = s_j^2 - s_i^2`` (``eps = (1e-12 s_max^2)^2``);
+  broadened ``F_ij = D / (D^2 + eps_ij)``, ``D = s_j^2 - s_i^2``,
+  ``eps_ij = (1e-8 max(s_i^2, s_j^2))^2``: inside an exactly degenerate multiplet -- lossy
+  single photons give many -- J - J^H vanishes in exact arithmetic, and the broadening
+  keeps its rounding from being multiplied by 1 / D; being relative to the pair, it leaves
+  the coupling of a small kept singular value to the zero ones (rank-deficient sectors)
+  intact;
 * contraction: ``Gamma_L_bar[:, q] += (Cbar o conj(w_q)) Gamma_R[q, :]^H``,
   ``Gamma_R_bar[q, :] += Gamma_L[:, q]^H (Cbar o conj(w_q))``, and the gate weights' gradient
   from the block sums of ``Cbar o conj(Gamma_L[:, q] Gamma_R[q, :])``, turned into
@@ -108,7 +113,7 @@ def sector_range(st, m):
     return lo0, hi0, lo1, hi1
 
 
-def svd_backward(theta, V, Vbar, Sbar, eps_rel=1e-12):
+def svd_backward(theta, V, Vbar, Sbar, eps_rel=1e-8):
     """Adjoint of the truncated thin SVD: gradient of theta (m x n) given the gradients of
     the kept left vectors (Vbar, m x k; V = the forward's kept vectors) and of the kept
     singular values (Sbar, k).  Uses the whole thin spectrum of theta, so the discarded
@@ -116,25 +121,27 @@ def svd_backward(theta, V, Vbar, Sbar, eps_rel=1e-12):
     torch = _torch()
     m, k = V.shape
     if theta.is_cuda:
-        U, S, Yh = torch.linalg.svd(theta, full_matrices=False, driver="gesvd")
+        U, S, Yh = torch.linalg.svd(theta, full_matrices=False, driver="gesvdj")
     else:
         U, S, Yh = torch.linalg.svd(theta, full_matrices=False)
     r = S.shape[0]
     Y = Yh.conj().transpose(0, 1).contiguous()
     U = U.contiguous()
     if k:
-        # the forward's gauge on the kept columns (u_i -> u_i ph_i, y_i -> y_i ph_i)
-        ph = (U[:, :k].conj() * V).sum(0)
-        ph = ph / ph.abs().clamp_min(1e-300)
+        # the kept columns are the forward's vectors, their right vectors y_i = theta^H v_i
+        # / s_i (inside a degenerate multiplet the forward's basis need not be the SVD's)
         U[:, :k] = V
-        Y[:, :k] = Y[:, :k] * ph[None, :]
+        Y[:, :k] = (theta.conj().transpose(0, 1) @ V) / S[:k][None, :].to(theta.dtype)
     Ub = torch.zeros((m, r), dtype=theta.dtype, device=theta.device)
     Ub[:, :k] = Vbar
     J = U.conj().transpose(0, 1) @ Ub
     s2 = S * S
     D = s2[None, :] - s2[:, None]                   # s_j^2 - s_i^2
-    eps = (eps_rel * float(s2.max())) ** 2 if r else 0.0
-    F = D / (D * D + eps)
+    # broadening relative to the pair's own scale: it damps near-degenerate pairs only,
+    # not the coupling of a small kept singular value to the (near-)zero ones
+    eps = (eps_rel * torch.maximum(s2[None, :], s2[:, None])) ** 2
+    den = D * D + eps
+    F = torch.where(den > 0, D / torch.where(den > 0, den, torch.ones_like(den)), torch.zeros_like(D))
     F.fill_diagonal_(0.0)
     core = (F * (J - J.conj().transpose(0, 1))) * S[None, :].to(theta.dtype)
     core = core + torch.diag(torch.cat([Sbar, Sbar.new_zeros(r - k)]).to(theta.dtype))
@@ -163,18 +170,35 @@ def update_backward(before, after, m, U3, Gbar, Lbar):
     tensor U3 (device complex128 [d, d, d]).  Gbar [n, chi, chi] and Lbar [n-1, chi]
     (device) hold the gradients with respect to the state after the update; on return
     they hold those with respect to the state before it.  Returns the gradient of the
-    gate tensor (device complex128 [d, d, d])."""
+    gate tensor (device complex128 [d, d, d]).
+
+    Dense per centre block q: Gamma_L with the columns outside q zeroed (GLq), Gamma_R
+    with the rows outside q zeroed (GRq), X_q = GLq GRq; a sector's weights w_q expanded to
+    chi x chi from the rows' and columns' charge blocks (zero outside the sector)."""
     torch = _torch()
     d, chi, n = before.d, before.chi, before.n
     dev, ct = before.G.device, before.G.dtype
+    nb = d * d
     GL, GR = before.G[m], before.G[m + 1]
     lamR = before.lam_dev(m + 2)
     CL, CR = before.charge[m], before.charge[m + 2]
     vL, vR = before.valid(m), before.valid(m + 2)
     qb = _qblocks(before, m)
-    X = [GL[:, idx] @ GR[idx, :] for (_, _, idx) in qb]
+    if not qb:
+        return torch.zeros((d, d, d), dtype=ct, device=dev)
+    qids = [q0 * d + q1 for (q0, q1, _) in qb]
+    cmask = torch.zeros((len(qb), chi), dtype=ct, device=dev)
+    for t, (_, _, cidx) in enumerate(qb):
+        cmask[t, cidx] = 1.0
+    GLq = GL[None, :, :] * cmask[:, None, :]
+    GRq = GR[None, :, :] * cmask[:, :, None]
+    X = GLq @ GRq                                   # [Q, chi, chi]
+    GLqH = GLq.conj().transpose(1, 2)
+    GRqH = GRq.conj().transpose(1, 2)
+    blkL = np.where(vL, CL[:, 0] * d + CL[:, 1], nb).astype(np.int64)
+    blkR = np.where(vR, CR[:, 0] * d + CR[:, 1], nb).astype(np.int64)
     # outputs of the forward and the incoming gradients
-    GLp, GRp = after.G[m], after.G[m + 1]
+    GLp = after.G[m]
     CCp, vCp = after.charge[m + 1], after.valid(m + 1)
     GbL, GbR = Gbar[m].clone(), Gbar[m + 1].clone()
     Sb_all = Lbar[m].clone() if 0 < m + 1 < n else None
@@ -188,8 +212,9 @@ def update_backward(before, after, m, U3, Gbar, Lbar):
     lo0, hi0, lo1, hi1 = sector_range(before, m)
     for cc0 in range(lo0, hi0 + 1):
         for cc1 in range(lo1, hi1 + 1):
-            l_idx = np.nonzero(vL & (CL[:, 0] >= cc0) & (CL[:, 1] >= cc1))[0]
-            r_idx = np.nonzero(vR & (CR[:, 0] <= cc0) & (CR[:, 1] <= cc1))[0]
+            inL = vL & (CL[:, 0] >= cc0) & (CL[:, 1] >= cc1)
+            inR = vR & (CR[:, 0] <= cc0) & (CR[:, 1] <= cc1)
+            l_idx, r_idx = np.nonzero(inL)[0], np.nonzero(inR)[0]
             if not len(l_idx) or not len(r_idx):
                 continue
             slots = np.nonzero(vCp & (CCp[:, 0] == cc0) & (CCp[:, 1] == cc1))[0]
@@ -199,51 +224,39 @@ def update_backward(before, after, m, U3, Gbar, Lbar):
             ri = torch.as_tensor(r_idx, device=dev)
             sl = torch.as_tensor(slots, device=dev)
             wb, ok, i0, i1 = _block_weights(U3h, d, cc0, cc1)
-            ablk = torch.as_tensor((CL[l_idx, 0] * d + CL[l_idx, 1]).astype(np.int64), device=dev)
-            bblk = torch.as_tensor((CR[r_idx, 0] * d + CR[r_idx, 1]).astype(np.int64), device=dev)
-            wb_dev = torch.as_tensor(wb, device=dev)
+            wbx = np.zeros((nb + 1, len(qids), nb + 1), dtype=np.complex128)
+            wbx[:nb, :, :nb] = wb[:, qids, :]
+            wbx_d = torch.as_tensor(wbx, device=dev)
+            rb = torch.as_tensor(np.where(inL, blkL, nb), device=dev)
+            cb = torch.as_tensor(np.where(inR, blkR, nb), device=dev)
+            Om = wbx_d[rb][:, :, cb].permute(1, 0, 2)   # [Q, chi, chi]
             # forward recompute of the sector
-            ws, C = [], torch.zeros((len(l_idx), len(r_idx)), dtype=ct, device=dev)
-            for t, (q0, q1, cidx) in enumerate(qb):
-                q = q0 * d + q1
-                if not ok[:, q, :].any():
-                    ws.append(None)
-                    continue
-                w = wb_dev[:, q, :][ablk][:, bblk]
-                ws.append(w)
-                C = C + X[t][li][:, ri] * w
+            C = (X * Om).sum(0)[li][:, ri]
             theta = C * lamR[ri][None, :]
             # gradients of the outputs: Gamma_L' = V, Gamma_R' = V^H C, Lambda' = S
             V = GLp[li][:, sl]
             Wb = GbR[sl][:, ri]
             Vb = GbL[li][:, sl] + C @ Wb.conj().transpose(0, 1)
             Sb = Sb_all[sl] if Sb_all is not None else torch.zeros(len(slots), dtype=torch.float64, device=dev)
-            Cb = V @ Wb
             tb = svd_backward(theta, V, Vb, Sb)
-            Cb = Cb + tb * lamR[ri][None, :]
+            Cb = V @ Wb + tb * lamR[ri][None, :]
             gLR.index_add_(0, ri, (tb.conj() * C).real.sum(0))
             # contraction adjoint
-            Ra = torch.nn.functional.one_hot(ablk, d * d).to(ct)
-            Rb = torch.nn.functional.one_hot(bblk, d * d).to(ct)
-            for t, (q0, q1, cidx) in enumerate(qb):
-                w = ws[t]
-                if w is None:
-                    continue
-                q = q0 * d + q1
-                Cw = Cb * w.conj()
-                gGL.index_put_((li[:, None], cidx[None, :]), Cw @ GR[cidx][:, ri].conj().transpose(0, 1),
-                               accumulate=True)
-                gGR.index_put_((cidx[:, None], ri[None, :]), GL[li][:, cidx].conj().transpose(0, 1) @ Cw,
-                               accumulate=True)
-                # gradient of the block weights: block sums of Cbar o conj(X_q)
-                wbar_dev.append(Ra.transpose(0, 1) @ (Cb * X[t][li][:, ri].conj()) @ Rb)
-                wbar_meta.append((ok[:, q, :], i0[:, q, :], i1[:, q, :]))
-    if wbar_dev:
-        allw = torch.stack(wbar_dev).cpu().numpy()
-        for wbar, (okq, i0q, i1q) in zip(allw, wbar_meta):
-            u0, u1 = u_flat[i0q], u_flat[i1q]
-            np.add.at(ubar, i0q[okq], (wbar * u1)[okq])
-            np.add.at(ubar, i1q[okq], (np.conj(wbar) * u0)[okq])
+            Cbf = torch.zeros((chi, chi), dtype=ct, device=dev)
+            Cbf[li[:, None], ri[None, :]] = Cb
+            Cw = Cbf[None] * Om.conj()
+            gGL += (Cw @ GRqH).sum(0)
+            gGR += (GLqH @ Cw).sum(0)
+            Ra = torch.nn.functional.one_hot(rb, nb + 1).to(ct)
+            Rc = torch.nn.functional.one_hot(cb, nb + 1).to(ct)
+            wbar_dev.append((Ra.transpose(0, 1)[None] @ (Cbf[None] * X.conj()) @ Rc[None])[:, :nb, :nb])
+            wbar_meta.append((ok[:, qids, :], i0[:, qids, :], i1[:, qids, :]))
+    for wq, (okq, i0q, i1q) in zip([w.cpu().numpy() for w in wbar_dev], wbar_meta):
+        # wq, okq, i0q, i1q: [a, Q, b] after the transpose below
+        wq = wq.transpose(1, 0, 2)
+        u0, u1 = u_flat[i0q], u_flat[i1q]
+        np.add.at(ubar, i0q[okq], (wq * u1)[okq])
+        np.add.at(ubar, i1q[okq], (np.conj(wq) * u0)[okq])
     Gbar[m] = gGL
     Gbar[m + 1] = gGR
     if 0 < m + 1 < n:

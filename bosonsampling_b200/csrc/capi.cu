@@ -1479,6 +1479,13 @@ int bsmpo_create(int n, int d, int chi, int flags, bsmpo_ctx** out) {
   // keep released workspace memory in the pool (no release at synchronisation points)
   uint64_t keep = UINT64_MAX;
   cudaMemPoolSetAttribute(h->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  // a block freed on one worker's stream is not handed to another worker's allocation
+  // with a hidden dependency on the first stream's pending work (which would serialise
+  // concurrent updates whenever a workspace grows); such blocks are reused once their
+  // free is known to be complete
+  int no = 0;
+  cudaMemPoolSetAttribute(h->pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+  cudaMemPoolSetAttribute(h->pool, cudaMemPoolReuseAllowOpportunistic, &no);
   h->cnt.assign((size_t)(n + 1) * d * d, 0);
   const char* prof = std::getenv("BSMPO_PROFILE");
   h->profile = prof && prof[0] == '1';
