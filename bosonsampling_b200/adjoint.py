@@ -11,7 +11,8 @@ hand-derived adjoint of that update, run on the device:
 
 * gauge: ``Gamma_L' Gamma_R' = V V^H C`` and ``Lambda'`` do not depend on the phases of the
   kept vectors, so the loss is gauge invariant and the adjoint needs no gauge term;
-* SVD: with ``U`` the left vectors (kept ones = the forward's ``V``), ``J = U^H Ubar``,
+* SVD: with ``U`` the exact left vectors (the forward's kept ``V = U_k R``, so
+  ``Ubar_k = Vbar R^H``), ``J = U^H Ubar``,
   ``theta_bar = U [(F o (J - J^H)) S + diag(Sbar)] Y^H + (I - U U^H) Ubar S^-1 Y^H`` over the
   whole thin spectrum (the discarded vectors enter through F), with the Lorentzian-
   broadened ``F_ij = D / (D^2 + eps_ij)``, ``D = s_j^2 - s_i^2``,
@@ -127,13 +128,15 @@ def svd_backward(theta, V, Vbar, Sbar, eps_rel=1e-8):
     r = S.shape[0]
     Y = Yh.conj().transpose(0, 1).contiguous()
     U = U.contiguous()
-    if k:
-        # the kept columns are the forward's vectors, their right vectors y_i = theta^H v_i
-        # / s_i (inside a degenerate multiplet the forward's basis need not be the SVD's)
-        U[:, :k] = V
-        Y[:, :k] = (theta.conj().transpose(0, 1) @ V) / S[:k][None, :].to(theta.dtype)
     Ub = torch.zeros((m, r), dtype=theta.dtype, device=theta.device)
-    Ub[:, :k] = Vbar
+    if k:
+        # the forward's kept vectors in the SVD's basis, V = U_k R: its phases, its basis
+        # inside degenerate multiplets, and the mixing of neighbouring small singular
+        # vectors that an iterative forward leaves at the rounding level; the gradient
+        # with respect to U_k is then Vbar R^H, and the formula below runs on the exact,
+        # orthonormal singular vectors
+        R = U[:, :k].conj().transpose(0, 1) @ V
+        Ub[:, :k] = Vbar @ R.conj().transpose(0, 1)
     J = U.conj().transpose(0, 1) @ Ub
     s2 = S * S
     D = s2[None, :] - s2[:, None]                   # s_j^2 - s_i^2
@@ -147,7 +150,8 @@ def svd_backward(theta, V, Vbar, Sbar, eps_rel=1e-8):
     core = core + torch.diag(torch.cat([Sbar, Sbar.new_zeros(r - k)]).to(theta.dtype))
     g = U @ core @ Y.conj().transpose(0, 1)
     if m > r and k:
-        P = Vbar - U @ (U.conj().transpose(0, 1) @ Vbar)
+        Ubk = Ub[:, :k]
+        P = Ubk - U @ (U.conj().transpose(0, 1) @ Ubk)
         g = g + (P / S[:k][None, :].to(theta.dtype)) @ Y[:, :k].conj().transpose(0, 1)
     return g
 
