@@ -615,7 +615,7 @@ def main():
 
     # ---- differentiation form: gradients of the squared distance between the marginals
     # of one circuit and those of a second Haar circuit, with respect to every (theta,
-    # phi) and eta, from the adjoint with checkpoints every 4 layers; checked against
+    # phi) and eta, from the adjoint over the recorded updates; checked against
     # central finite differences of the library's forward (h = 1e-6, FP64)
     grad = None
     if not args.no_grad and not args.bs_slice and world == 1:
@@ -626,7 +626,7 @@ def main():
         photons = list(range(0, gn, 2))
         gth = np.array([b[2] for b in gbs])
         gphi = np.array([b[3] for b in gbs])
-        circ = adjoint.DiffCircuit(gn, gd, gchi, photons, gbs, gph, checkpoint_layers=4)
+        circ = adjoint.DiffCircuit(gn, gd, gchi, photons, gbs, gph)
         tc = adjoint.DiffCircuit(gn, gd, gchi, photons, tbs, tph)
         ttr, tP = tc.run(np.array([b[2] for b in tbs]), np.array([b[3] for b in tbs]), geta)
         tc.close()
@@ -671,11 +671,12 @@ def main():
         grad = {"config": "N=24, 12 photons (even modes), eta=0.5, d=4, chi=256, Haar seed %d -> %d-BS mesh; "
                           "target: marginals of Haar seed %d" % (gseed, nb, gseed + 1),
                 "loss": gl, "params": 2 * nb + 1, "forward_seconds": round(t_fwd, 3),
-                "loss_and_grad_seconds": round(t_grad, 3), "checkpoint_layers": 4,
+                "loss_and_grad_seconds": round(t_grad, 3), "records": "two sites and three bonds per update",
                 "peak_device_bytes": int(peak), "fd_check": checks, "fd_max_rel_err": max(errs),
-                "how": "library forward (plain FP64 path), MPO checkpoints every 4 layers, each segment "
-                       "recomputed update by update; hand-written adjoint of the contraction + truncated "
-                       "SVD (Lorentzian-broadened F) on the device; gate angles by bsmpo_bs_angle_grad"}
+                "how": "library forward (plain FP64 path) update by update, keeping each update's inputs "
+                       "and outputs (two sites, three bonds); hand-written adjoint of the contraction + "
+                       "truncated SVD (pair-relative Lorentzian broadening) on the device; gate angles by "
+                       "bsmpo_bs_angle_grad"}
 
     # ---- roofline of the dominant phase: the SVD step (Jacobi rounds, or the Gram GEMM,
     # Householder reduction and bisection of the Gram route), FP64 against measured DGEMM

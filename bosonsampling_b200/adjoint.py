@@ -25,8 +25,8 @@ hand-derived adjoint of that update, run on the device:
   ``Gamma_R_bar[q, :] += Gamma_L[:, q]^H (Cbar o conj(w_q))``, and the gate weights' gradient
   from the block sums of ``Cbar o conj(Gamma_L[:, q] Gamma_R[q, :])``, turned into
   dL/dtheta, dL/dphi on the device (``bsmpo_bs_angle_grad``);
-* memory: the MPO is checkpointed every ``checkpoint_layers`` mesh layers; each segment is
-  recomputed update by update on the backward pass.
+* memory: the forward keeps, per update, the two sites and three bonds it reads and the
+  two sites and bond it writes (4 chi^2 complex numbers), not whole states.
 
 The loss, the output phases and the marginals are plain torch operations on the device
 (autograd glue); the initial product state's dependence on eta is the derivative of
@@ -365,6 +365,39 @@ def _t_matrix(theta, phi):
     return np.array([[e * c, -s], [e * s, c]], dtype=np.complex128)
 
 
+class _Sites:
+    """Two site tensors of a state, indexable by their site numbers."""
+
+    def __init__(self, tensors):
+        self._t = tensors
+        first = next(iter(tensors.values()))
+        self.device, self.dtype = first.device, first.dtype
+
+    def __getitem__(self, i):
+        return self._t[i]
+
+
+class _Piece:
+    """The part of a state that the update at mode m reads and writes: sites m, m+1 and
+    the bonds m, m+1, m+2 (the StateT interface of update_backward)."""
+
+    def __init__(self, st, m):
+        self.d, self.chi, self.n, self.m = st.d, st.chi, st.n, m
+        self.G = _Sites({m: st.G[m].clone(), m + 1: st.G[m + 1].clone()})
+        self.charge = {b: st.charge[b].copy() for b in (m, m + 1, m + 2)}
+        self._lam = {b: st.lam_dev(b).clone() for b in (m, m + 1, m + 2)}
+        self._lam_h = {b: st.lam_host(b).copy() for b in (m, m + 1, m + 2)}
+
+    def lam_dev(self, b):
+        return self._lam[b]
+
+    def lam_host(self, b):
+        return self._lam_h[b]
+
+    def valid(self, b):
+        return (self.charge[b][:, 0] < self.d) & (self._lam_h[b] > 0)
+
+
 class DiffCircuit:
     """A lossy-single-photon circuit whose output marginals are differentiable in every
     beam splitter's (theta, phi) and in eta.
@@ -372,15 +405,18 @@ class DiffCircuit:
     ``mesh``: (layer, mode, theta, phi) in circuit order (``interferometer.circuit``);
     ``phases``: the output phase screen (it leaves the marginals unchanged but is part of
     the forward).  The forward runs on the library (``precision``, default the plain FP64
-    path); ``checkpoint_layers`` mesh layers lie between two stored states."""
+    path), one update after another, keeping for each update the two sites and three
+    bonds it reads and the two sites and bond it writes (4 chi^2 complex numbers): the
+    backward needs the forward's own output basis -- inside degenerate multiplets of
+    singular values the library's result is not bitwise the same between its concurrent
+    and sequential schedules, so recomputing a segment from a stored MPO could hand the
+    adjoint a different (equally valid) basis than the one its incoming gradient refers to."""
 
-    def __init__(self, n, d, chi, photon_modes, mesh, phases, precision="fp64", workers=8,
-                 checkpoint_layers=4):
+    def __init__(self, n, d, chi, photon_modes, mesh, phases, precision="fp64", workers=8):
         self.n, self.d, self.chi = n, d, chi
         self.photon_modes = list(photon_modes)
         self.mesh = [(int(l), int(m)) for (l, m, _, _) in mesh]
         self.phases = np.asarray(phases, dtype=np.float64)
-        self.k = int(checkpoint_layers)
         self.sim = engine.MPOSimulator(n, d, chi)
         self.sim.set_precision(precision)
         self.sim.set_workers(workers)
@@ -401,30 +437,30 @@ class DiffCircuit:
         sim.apply_phases(self.phases)
         return sim.observables()
 
-    def _load(self, st):
-        self.sim.load(st.G, st.Lam, st.charge_dev)
-
     def _state(self):
         g, lam, c = self.sim.store()
-        st = StateT(g, lam, c, self.d)
-        st.charge_dev = c
-        return st
+        return StateT(g, lam, c, self.d)
 
     def forward_records(self, thetas, phis, eta):
-        """Runs the circuit keeping the product state, the checkpoints and the final state."""
+        """Runs the circuit update by update; returns the product state, the records
+        (mode, gate angles or None, before, after) of every update -- the canonicalising
+        sweep's and the mesh's -- and the final state."""
         sim = self.sim
         sim.init_single_photons(self.photon_modes, eta, canonicalize=False)
         prod = self._state()
-        sim.canonicalize()
-        ckpts = []
-        for L0 in range(0, len(self.layers), self.k):
-            ckpts.append(self._state())
-            for L in self.layers[L0:L0 + self.k]:
-                if L:
-                    sim.run_mesh([self.mesh[i][1] for i in L], [thetas[i] for i in L], [phis[i] for i in L])
-        return prod, ckpts, self._state()
+        cur = prod
+        recs = []
+        steps = [(m, None) for m in range(self.n - 2, -1, -1)]
+        steps += [(self.mesh[i][1], i) for L in self.layers for i in L]
+        for (m, i) in steps:
+            S = np.eye(2, dtype=np.complex128) if i is None else _t_matrix(thetas[i], phis[i])
+            before = _Piece(cur, m)
+            sim.bs_update(m, S)
+            cur = self._state()
+            recs.append((m, i, before, _Piece(cur, m)))
+        return prod, recs, cur
 
-    def backward(self, thetas, phis, eta, prod, ckpts, final, Gbar):
+    def backward(self, thetas, phis, eta, prod, recs, final, Gbar):
         """Gradients (theta [n_bs], phi [n_bs], eta) from Gbar = dL/dGamma of the final
         state (before the phase screen)."""
         torch = _torch()
@@ -433,31 +469,12 @@ class DiffCircuit:
         Gbar = Gbar.clone()
         Lbar = torch.zeros((n - 1, chi), dtype=torch.float64, device=dev)
         ubar = torch.zeros((len(self.mesh), d, d, d), dtype=torch.complex128, device=dev)
-        for j in range(len(ckpts) - 1, -1, -1):
-            ops = [i for L in self.layers[j * self.k:(j + 1) * self.k] for i in L]
-            self._load(ckpts[j])
-            recs = [ckpts[j]]
-            gates = []
-            for i in ops:
-                m = self.mesh[i][1]
-                self.sim.bs_update(m, _t_matrix(thetas[i], phis[i]))
-                recs.append(self._state())
-                gates.append(gate_tensor(d, thetas[i], phis[i], dev))
-            for t in range(len(ops) - 1, -1, -1):
-                i = ops[t]
-                ubar[i] = update_backward(recs[t], recs[t + 1], self.mesh[i][1], gates[t], Gbar, Lbar)
-            del recs
-        # the canonicalising sweep (identity gates, right to left)
-        self._load(prod)
-        recs = [prod]
         ident = identity_tensor(d, dev)
-        sweep = list(range(n - 2, -1, -1))
-        for m in sweep:
-            self.sim.bs_update(m, np.eye(2, dtype=np.complex128))
-            recs.append(self._state())
-        for t in range(len(sweep) - 1, -1, -1):
-            update_backward(recs[t], recs[t + 1], sweep[t], ident, Gbar, Lbar)
-        del recs
+        for (m, i, before, after) in reversed(recs):
+            u = ident if i is None else gate_tensor(d, thetas[i], phis[i], dev)
+            ub = update_backward(before, after, m, u, Gbar, Lbar)
+            if i is not None:
+                ubar[i] = ub
         # eta: the product state's entries are (1 - eta) at occupation (0, 0) and eta at
         # (1, 1) on the photon modes
         g_eta = 0.0
@@ -475,14 +492,14 @@ class DiffCircuit:
     def loss_and_grad(self, thetas, phis, eta, target):
         """(loss, dL/dtheta, dL/dphi, dL/deta) of the marginal loss against ``target``."""
         torch = _torch()
-        prod, ckpts, final = self.forward_records(thetas, phis, eta)
+        prod, recs, final = self.forward_records(thetas, phis, eta)
         G = final.G.clone().requires_grad_(True)
         f = phase_factors(final.charge, self.phases, self.d, G.device)
         tr, P = marginals_torch(G * f, final.charge, final.lam_host, self.d)
         tgt = torch.as_tensor(np.asarray(target, dtype=np.float64), device=G.device)
         loss = marginal_loss(P, tr, tgt)
         loss.backward()
-        g_th, g_ph, g_eta = self.backward(thetas, phis, eta, prod, ckpts, final, G.grad)
+        g_th, g_ph, g_eta = self.backward(thetas, phis, eta, prod, recs, final, G.grad)
         return float(loss.detach()), g_th, g_ph, g_eta
 
 
@@ -510,8 +527,8 @@ def _marginals_function():
                 th = thetas.detach().cpu().numpy().astype(np.float64)
                 ph = phis.detach().cpu().numpy().astype(np.float64)
                 e = float(eta.detach())
-                prod, ckpts, final = circuit.forward_records(th, ph, e)
-                ctx.saved = (circuit, th, ph, e, prod, ckpts, final)
+                prod, recs, final = circuit.forward_records(th, ph, e)
+                ctx.saved = (circuit, th, ph, e, prod, recs, final)
                 f = phase_factors(final.charge, circuit.phases, circuit.d, final.G.device)
                 with torch.no_grad():
                     tr, P = marginals_torch(final.G * f, final.charge, final.lam_host, circuit.d)
@@ -519,13 +536,13 @@ def _marginals_function():
 
             @staticmethod
             def backward(ctx, g_tr, g_P):
-                circuit, th, ph, e, prod, ckpts, final = ctx.saved
+                circuit, th, ph, e, prod, recs, final = ctx.saved
                 with torch.enable_grad():
                     G = final.G.clone().requires_grad_(True)
                     f = phase_factors(final.charge, circuit.phases, circuit.d, G.device)
                     tr, P = marginals_torch(G * f, final.charge, final.lam_host, circuit.d)
                     torch.autograd.backward([tr, P], [g_tr, g_P])
-                g_th, g_ph, g_eta = circuit.backward(th, ph, e, prod, ckpts, final, G.grad)
+                g_th, g_ph, g_eta = circuit.backward(th, ph, e, prod, recs, final, G.grad)
                 dev = g_P.device
                 return (g_th.to(dev), g_ph.to(dev), torch.tensor(g_eta, dtype=torch.float64, device=dev), None)
 

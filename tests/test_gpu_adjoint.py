@@ -53,7 +53,7 @@ def test_gate_angle_gradient_matches_finite_differences():
 def test_circuit_gradient_matches_torch_autograd_and_finite_differences(n, d, chi, seed):
     bs, ph, th, phi, target = _setup(n, d, chi, seed)
     photons, eta = list(range(0, n, 2)), 0.6
-    circ = adjoint.DiffCircuit(n, d, chi, photons, bs, ph, checkpoint_layers=2)
+    circ = adjoint.DiffCircuit(n, d, chi, photons, bs, ph)
     try:
         loss, g_th, g_ph, g_eta = circ.loss_and_grad(th, phi, eta, target)
         # the pure-torch FP64 autograd reference
@@ -90,25 +90,48 @@ def test_circuit_gradient_matches_torch_autograd_and_finite_differences(n, d, ch
         circ.close()
 
 
-def test_autograd_function_and_checkpoint_spacing_agree():
+def test_autograd_function_agrees_with_loss_and_grad():
     n, d, chi, seed = 6, 3, 12, 13
     bs, ph, th, phi, target = _setup(n, d, chi, seed)
-    photons = list(range(0, n, 2))
-    grads = []
-    for k in (1, 3):
-        circ = adjoint.DiffCircuit(n, d, chi, photons, bs, ph, checkpoint_layers=k)
-        try:
-            grads.append(circ.loss_and_grad(th, phi, 0.55, target)[1:])
-            if k == 3:
-                t_th = torch.tensor(th, dtype=torch.float64, device="cuda", requires_grad=True)
-                t_ph = torch.tensor(phi, dtype=torch.float64, device="cuda", requires_grad=True)
-                t_eta = torch.tensor(0.55, dtype=torch.float64, device="cuda", requires_grad=True)
-                trace, P = adjoint.CircuitMarginals.apply(t_th, t_ph, t_eta, circ)
-                ((P.real / trace.real - torch.as_tensor(target, device="cuda")) ** 2).sum().backward()
-                assert _rel(t_th.grad.cpu(), grads[-1][0].cpu()) < 1e-12
-                assert _rel(t_ph.grad.cpu(), grads[-1][1].cpu()) < 1e-12
-                assert abs(float(t_eta.grad) - grads[-1][2]) <= 1e-12 * max(1.0, abs(grads[-1][2]))
-        finally:
-            circ.close()
-    assert _rel(grads[0][0].cpu(), grads[1][0].cpu()) < 1e-12
-    assert _rel(grads[0][1].cpu(), grads[1][1].cpu()) < 1e-12
+    circ = adjoint.DiffCircuit(n, d, chi, list(range(0, n, 2)), bs, ph)
+    try:
+        _, g_th, g_ph, g_eta = circ.loss_and_grad(th, phi, 0.55, target)
+        t_th = torch.tensor(th, dtype=torch.float64, device="cuda", requires_grad=True)
+        t_ph = torch.tensor(phi, dtype=torch.float64, device="cuda", requires_grad=True)
+        t_eta = torch.tensor(0.55, dtype=torch.float64, device="cuda", requires_grad=True)
+        trace, P = adjoint.CircuitMarginals.apply(t_th, t_ph, t_eta, circ)
+        ((P.real / trace.real - torch.as_tensor(target, device="cuda")) ** 2).sum().backward()
+        assert _rel(t_th.grad.cpu(), g_th.cpu()) < 1e-12
+        assert _rel(t_ph.grad.cpu(), g_ph.cpu()) < 1e-12
+        assert abs(float(t_eta.grad) - g_eta) <= 1e-12 * max(1.0, abs(g_eta))
+    finally:
+        circ.close()
+
+
+def test_deep_circuit_early_parameters_match_finite_differences():
+    """N=24, d=4, chi=256, 8 layers (truncating, degenerate spectra at eta = 0.5): the
+    gradients of the first layer's angles and of eta pass through every later update."""
+    n, d, chi = 24, 4, 256
+    _, bs, ph = interferometer.circuit(n, 1005)
+    bs = [b for b in bs if b[0] < 8]
+    target = np.random.default_rng(0).dirichlet(np.ones(d), size=n)
+    th = np.array([b[2] for b in bs])
+    phi = np.array([b[3] for b in bs])
+    circ = adjoint.DiffCircuit(n, d, chi, list(range(0, n, 2)), bs, ph)
+    try:
+        _, g_th, g_ph, g_eta = circ.loss_and_grad(th, phi, 0.5, target)
+
+        def L(t, p, e):
+            trc, Pm = circ.run(t, p, e)
+            return float(((Pm.real / trc.real - target) ** 2).sum())
+        h = 1e-6
+        for i in (0, 1, len(th) // 2):
+            tp, tm = th.copy(), th.copy()
+            tp[i] += h
+            tm[i] -= h
+            fd = (L(tp, phi, 0.5) - L(tm, phi, 0.5)) / (2 * h)
+            assert abs(float(g_th[i]) - fd) <= 1e-5 * max(abs(fd), 1e-3)
+        fd = (L(th, phi, 0.5 + h) - L(th, phi, 0.5 - h)) / (2 * h)
+        assert abs(g_eta - fd) <= 1e-5 * max(abs(fd), 1e-3)
+    finally:
+        circ.close()
