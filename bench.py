@@ -663,16 +663,20 @@ def main():
             checks.append({"param": kind if kind == "eta" else "%s[%d]" % (kind, i), "adjoint": g,
                            "finite_difference": fd})
         circ.close()
-        # relative to each finite difference, floored at 1e-3 of the largest one checked
+        # relative to each finite difference where it is significant (>= 1e-3 of the largest
+        # one checked); for the others the absolute difference against that scale, which
+        # the finite difference's own rounding (~1e-16 loss / h) bounds from below
         scale = max(abs(fd) for _, fd in errs)
         for c, (g, fd) in zip(checks, errs):
-            c["rel_err"] = abs(g - fd) / max(abs(fd), 1e-3 * scale)
-        errs = [c["rel_err"] for c in checks]
+            c["rel_err"] = abs(g - fd) / abs(fd) if abs(fd) >= 1e-3 * scale else None
+            c["abs_err_over_scale"] = abs(g - fd) / scale
+        errs = [c["rel_err"] for c in checks if c["rel_err"] is not None]
         grad = {"config": "N=24, 12 photons (even modes), eta=0.5, d=4, chi=256, Haar seed %d -> %d-BS mesh; "
                           "target: marginals of Haar seed %d" % (gseed, nb, gseed + 1),
                 "loss": gl, "params": 2 * nb + 1, "forward_seconds": round(t_fwd, 3),
                 "loss_and_grad_seconds": round(t_grad, 3), "records": "two sites and three bonds per update",
                 "peak_device_bytes": int(peak), "fd_check": checks, "fd_max_rel_err": max(errs),
+                "fd_max_abs_err_over_scale": max(c["abs_err_over_scale"] for c in checks),
                 "how": "library forward (plain FP64 path) update by update, keeping each update's inputs "
                        "and outputs (two sites, three bonds); hand-written adjoint of the contraction + "
                        "truncated SVD (pair-relative Lorentzian broadening) on the device; gate angles by "
