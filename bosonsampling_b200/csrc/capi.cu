@@ -207,7 +207,10 @@ int grow(bsmpo_ctx* h, DevBuf& b, size_t bytes) {
   if (b.p) CK(h, cudaFreeAsync(b.p, h->stream));
   b.p = nullptr;
   b.bytes = 0;
-  size_t want = align_up(bytes + bytes / 4 + 256, 256);
+  // the next power of two: a buffer grows at most a few times however its sectors grow
+  // (a growth inside a timed layer costs a pool allocation on the worker's stream)
+  size_t want = 4096;
+  while (want < bytes + 256) want <<= 1;
   h->dev_grows++;
   if (cudaMallocFromPoolAsync(&b.p, want, h->pool, h->stream) != cudaSuccess) {
     cudaGetLastError();
