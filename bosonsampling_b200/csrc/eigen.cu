@@ -35,21 +35,17 @@ namespace cg = cooperative_groups;
 namespace {
 
 constexpr double EPS = 2.220446049250313e-16;
-// threads per CTA of the tridiagonalisation and its minimum resident CTAs per SM
-// (compile-time tuning constants; measured at chi = 1024 with 16 concurrent updates:
-// 128 x 6 gives 558-564 BS-updates/s, 256 x 3 516-528, 512 x 2 467-501 -- the stage is
-// limited by resident CTA slots shared by the concurrent updates, not by one update's
-// latency)
-#ifndef BSMPO_TD_NT
-#define BSMPO_TD_NT 128
-#endif
-#ifndef BSMPO_TD_MINB
-#define BSMPO_TD_MINB 6
-#endif
-constexpr int TD_NT = BSMPO_TD_NT;
+// Threads per CTA of the tridiagonalisation: two instantiations, 128 threads (6 CTAs per
+// SM by registers) for the small size classes and 256 threads (2 per SM) for the classes
+// from BSMPO_TD_WIDE on (0-4, default 4: none).  Measured at chi = 1024 with 16
+// concurrent updates: 256 threads for every class 656-672 BS-updates/s against 733-744
+// for none; for the classes with k > 320 only (BSMPO_TD_WIDE=2) 760-776 against 790-793
+// in the same run -- the wider CTAs shorten the largest sector's chain but cost resident
+// CTA slots the concurrent updates share.
+constexpr int TD_NT = 128;
+constexpr int TD_NT_WIDE = 256;
 constexpr int TD_CLASSES = 4;   // cluster sizes 1, 2, 4, 8 CTAs per sector, by sector size
-
-constexpr int TD_NW = TD_NT / 32;   // warps per CTA, each streaming its own rows
+constexpr int TD_NW_MAX = TD_NT_WIDE / 32;
 // bulk-copy ring of each warp: about BSMPO_TD_RING_KB per CTA, 1, 2 or TD_MAXSLOT row
 // slots (pairs of rows share one pass over the vectors)
 #ifndef BSMPO_TD_RING_KB
@@ -59,30 +55,31 @@ constexpr int TD_MAXSLOT = 4;
 #ifndef BSMPO_TD_PAIRS
 #define BSMPO_TD_PAIRS 1   // rows two at a time (0: one at a time)
 #endif
-static_assert(TD_NW >= 1 && TD_NW <= 8 && (TD_NW & (TD_NW - 1)) == 0,
-              "the tridiagonalisation takes 1, 2, 4 or 8 warps per CTA");
+static_assert(TD_NW_MAX <= 8, "the per-warp scalars of the tridiagonalisation hold 8 warps");
 
 // shared memory of the tridiagonalisation with `slots` ring slots per warp (kmax = the
 // launch's largest k, cl = CTAs per sector): the row rings, v and w of two steps, the
 // published and the copied row, p of the own rows (two steps), 64 scalars and the rings'
 // mbarriers
-__host__ __device__ inline size_t td_smem_for(int kmax, int cl, int slots) {
+__host__ __device__ inline size_t td_smem_for(int kmax, int cl, int slots, int nw) {
   const int own = kmax / cl + 1;
-  return sizeof(cplx) * ((size_t)TD_NW * slots * kmax + 6 * (size_t)kmax + 2 * (size_t)own) +
-         64 * sizeof(double) + TD_NW * TD_MAXSLOT * sizeof(uint64_t);
+  return sizeof(cplx) * ((size_t)nw * slots * kmax + 6 * (size_t)kmax + 2 * (size_t)own) +
+         64 * sizeof(double) + nw * TD_MAXSLOT * sizeof(uint64_t);
 }
 
 // ring slots per warp: a power of two, 2 to TD_MAXSLOT within about BSMPO_TD_RING_KB per
 // CTA, fewer where a one-CTA sector of size kmax would not fit in 227 KB
-__host__ __device__ inline int td_slots(int kmax) {
-  const long long fit = (long long)BSMPO_TD_RING_KB * 1024 / ((long long)TD_NW * kmax * (long long)sizeof(cplx));
+__host__ __device__ inline int td_slots(int kmax, int nw) {
+  const long long fit = (long long)BSMPO_TD_RING_KB * 1024 / ((long long)nw * kmax * (long long)sizeof(cplx));
   int s = fit >= TD_MAXSLOT ? TD_MAXSLOT : 2;
-  while (s > 1 && td_smem_for(kmax, 1, s) > 227 * 1024) s >>= 1;
+  while (s > 1 && td_smem_for(kmax, 1, s, nw) > 227 * 1024) s >>= 1;
   return s;
 }
 
-// dynamic shared memory of a tridiagonalisation launch
-__host__ __device__ inline size_t td_smem_bytes(int kmax, int cl) { return td_smem_for(kmax, cl, td_slots(kmax)); }
+// dynamic shared memory of a tridiagonalisation launch with nw warps per CTA
+__host__ __device__ inline size_t td_smem_bytes(int kmax, int cl, int nw) {
+  return td_smem_for(kmax, cl, td_slots(kmax, nw), nw);
+}
 
 __device__ __forceinline__ cplx warp_sum(cplx v) {
 #pragma unroll
@@ -147,10 +144,13 @@ __device__ __forceinline__ cplx cdiv(cplx a, cplx b) {
 //    -- instead of one L2 round trip per load.  A row is read and written by one warp
 //    only; its write-back is ordered before the next bulk read of it by a proxy fence
 //    of the writing lanes and the warp's synchronisation.
-__global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
+template <int TD_NT_, int MINB>
+__global__ void __launch_bounds__(TD_NT_, MINB)
     tridiag_kernel(const SectorDesc* __restrict__ sd, const int* __restrict__ list, int kmax,
                    cplx* __restrict__ gbuf, double* __restrict__ dbuf, double* __restrict__ ebuf,
                    cplx* __restrict__ taubuf, int* __restrict__ err) {
+  constexpr int TD_NT = TD_NT_;        // threads of this instantiation
+  constexpr int TD_NW = TD_NT_ / 32;   // its warps, each streaming its own rows
   extern __shared__ __align__(128) unsigned char smem_raw[];
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(TD_NT, BSMPO_TD_MINB)
   const int cls = __ffs(TD_CL) - 1;                // log2 of it
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int own_cap = kmax / TD_CL + 1;
-  const int nslot = td_slots(kmax);                 // 1, 2 or 4
+  const int nslot = td_slots(kmax, TD_NW);         // 1, 2 or 4
   const int nss = __ffs(nslot) - 1;
   cplx* ring = reinterpret_cast<cplx*>(smem_raw);  // slot s of warp w: ring + (w nslot + s) kmax
   cplx* vb = ring + (size_t)TD_NW * nslot * kmax;  // v of two consecutive steps: vb + (j & 1) kmax
@@ -718,7 +718,7 @@ int eigen_max_k() {
   static const int kmax = [] {
     int best = 0;
     for (int k = 1; k <= 32 * 32; ++k) {   // the back-transformation keeps 32 entries per lane
-      if (td_smem_bytes(k, 1) > 227 * 1024) break;
+      if (td_smem_bytes(k, 1, TD_NT / 32) > 227 * 1024) break;
       best = k;
     }
     return best;
@@ -746,11 +746,23 @@ cudaError_t launch_tridiag(const SectorDesc* sd_dev, const int* list_dev, const 
                            void* taubuf, int* err, const cudaStream_t* streams) {
   // once per process: the largest dynamic shared memory any launch may ask for
   static const cudaError_t attr = [] {
-    size_t most = 0;
-    for (int k = 1; k <= eigen_max_k(); ++k) most = std::max(most, td_smem_bytes(k, 1));
-    return cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most);
+    size_t most = 0, most_w = 0;
+    for (int k = 1; k <= eigen_max_k(); ++k) {
+      most = std::max(most, td_smem_bytes(k, 1, TD_NT / 32));
+      const size_t w = td_smem_bytes(k, 1, TD_NT_WIDE / 32);
+      if (w <= 227 * 1024) most_w = std::max(most_w, w);
+    }
+    cudaError_t e = cudaFuncSetAttribute(tridiag_kernel<TD_NT, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(tridiag_kernel<TD_NT_WIDE, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most_w);
+    return e;
   }();
   if (attr != cudaSuccess) return attr;
+  // the first size class on 256-thread CTAs (BSMPO_TD_WIDE, 0-4; 4: none), read once
+  static const int wide = [] {
+    const char* e = std::getenv("BSMPO_TD_WIDE");
+    return (e && e[0] >= '0' && e[0] <= '4') ? e[0] - '0' : TD_CLASSES;
+  }();
   int first = 0;
   for (int c = 0; c < TD_CLASSES; ++c) {
     const int count = class_count[c];
@@ -758,8 +770,11 @@ cudaError_t launch_tridiag(const SectorDesc* sd_dev, const int* list_dev, const 
     const int cl = 1 << c;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(count * cl);
-    cfg.blockDim = dim3(TD_NT);
-    cfg.dynamicSmemBytes = td_smem_bytes(class_kmax[c], cl);
+    // 256 threads where asked and where their larger rings fit the launch's shared memory
+    const bool w = c >= wide && td_smem_bytes(class_kmax[c], 1, TD_NT_WIDE / 32) <= 227 * 1024;
+    const int nt = w ? TD_NT_WIDE : TD_NT;
+    cfg.blockDim = dim3(nt);
+    cfg.dynamicSmemBytes = td_smem_bytes(class_kmax[c], cl, nt / 32);
     cfg.stream = streams[TD_CLASSES - 1 - c];   // the largest class on the caller's stream
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -768,9 +783,12 @@ cudaError_t launch_tridiag(const SectorDesc* sd_dev, const int* list_dev, const 
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, tridiag_kernel, sd_dev, list_dev + first, class_kmax[c],
-                                       reinterpret_cast<cplx*>(gbuf), dbuf, ebuf,
-                                       reinterpret_cast<cplx*>(taubuf), err);
+    cudaError_t e = w ? cudaLaunchKernelEx(&cfg, tridiag_kernel<TD_NT_WIDE, 2>, sd_dev, list_dev + first,
+                                           class_kmax[c], reinterpret_cast<cplx*>(gbuf), dbuf, ebuf,
+                                           reinterpret_cast<cplx*>(taubuf), err)
+                      : cudaLaunchKernelEx(&cfg, tridiag_kernel<TD_NT, 6>, sd_dev, list_dev + first,
+                                           class_kmax[c], reinterpret_cast<cplx*>(gbuf), dbuf, ebuf,
+                                           reinterpret_cast<cplx*>(taubuf), err);
     if (e != cudaSuccess) return e;
     first += count;
   }
