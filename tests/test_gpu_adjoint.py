@@ -63,7 +63,8 @@ def test_circuit_gradient_matches_torch_autograd_and_finite_differences(n, d, ch
         trace, P = tr.circuit(n, d, chi, photons, t_eta, bs, t_th, t_ph, ph)
         ref_loss = ((P.real / trace.real - torch.as_tensor(target)) ** 2).sum()
         ref_loss.backward()
-        assert abs(loss - float(ref_loss)) <= 1e-10 * max(1.0, abs(float(ref_loss)))
+        ref = float(ref_loss.detach())
+        assert abs(loss - ref) <= 1e-10 * max(1.0, abs(ref))
         assert _rel(g_th.cpu(), t_th.grad) < 1e-6
         assert _rel(g_ph.cpu(), t_ph.grad) < 1e-6
         assert abs(g_eta - float(t_eta.grad)) <= 1e-6 * max(1.0, abs(float(t_eta.grad)))
