@@ -36,6 +36,10 @@ SIGNATURES = {
     "bsmpo_set_workers": (_c_int, [_vp, _c_int]),
     "bsmpo_load_state": (_c_int, [_vp, _vp, _vp, _vp]),
     "bsmpo_store_state": (_c_int, [_vp, _vp, _vp, _vp]),
+    "bsmpo_get_site": (_c_int, [_vp, _c_int, _vp]),
+    "bsmpo_put_site": (_c_int, [_vp, _c_int, _vp]),
+    "bsmpo_get_bond": (_c_int, [_vp, _c_int, _vp, _vp]),
+    "bsmpo_put_bond": (_c_int, [_vp, _c_int, _vp, _vp]),
     "bsmpo_init_product": (_c_int, [_vp, _dp, _c_int]),
     "bsmpo_canonicalize": (_c_int, [_vp]),
     "bsmpo_bs_update": (_c_int, [_vp, _c_int, _dp]),

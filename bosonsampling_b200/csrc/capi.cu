@@ -1552,33 +1552,42 @@ int bsmpo_set_cutoff(bsmpo_ctx* h, double cutoff) {
 // Validates the charges and Lambda of a state (host copies: hc [(n+1) chi][2], hl
 // [(n+1) chi] with the inner bonds filled) and rebuilds the host mirror of the block
 // sizes; fills the edge Lambda of hl (1 on the occupied slots of bonds 0 and n).
+// Checks one bond (host copies: hc [chi][2], hl [chi]; hl is not read on the edge bonds 0
+// and n) and writes its block sizes to row [d*d]: sorted, occupied slots first, charges in
+// range, Lambda > 0 on the occupied slots and 0 on the empty ones.
+int validate_bond(bsmpo_ctx* h, int b, const int* hc, const double* hl, int* row) {
+  const int n = h->n, d = h->d, chi = h->chi;
+  std::fill(row, row + d * d, 0);
+  bool empty_seen = false;
+  int p0 = -1, p1 = -1;
+  for (int i = 0; i < chi; ++i) {
+    const int c0 = hc[(size_t)i * 2], c1 = hc[(size_t)i * 2 + 1];
+    const bool occ = c0 < d;
+    if (!occ) {
+      if (c0 != d || c1 != d)
+        return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": empty slots must carry (d, d)");
+      empty_seen = true;
+      if (b > 0 && b < n && hl[i] != 0.0)
+        return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": Lambda on an empty slot");
+      continue;
+    }
+    if (empty_seen) return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": occupied slot after an empty one");
+    if (c0 < 0 || c1 < 0 || c1 >= d) return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": charge out of range");
+    if (c0 < p0 || (c0 == p0 && c1 < p1))
+      return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": charges not sorted");
+    if (b > 0 && b < n && !(hl[i] > 0.0))
+      return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": occupied slot with Lambda <= 0");
+    p0 = c0; p1 = c1;
+    row[c0 * d + c1]++;
+  }
+  return BSMPO_OK;
+}
+
 int validate_state(bsmpo_ctx* h, const int* hc, double* hl) {
   const int n = h->n, d = h->d, chi = h->chi;
-  // sorted, occupied slots first, charges in range, Lambda > 0 on occupied slots
-  std::fill(h->cnt.begin(), h->cnt.end(), 0);
   for (int b = 0; b <= n; ++b) {
-    bool empty_seen = false;
-    int p0 = -1, p1 = -1;
-    for (int i = 0; i < chi; ++i) {
-      const int c0 = hc[((size_t)b * chi + i) * 2], c1 = hc[((size_t)b * chi + i) * 2 + 1];
-      const bool occ = c0 < d;
-      if (!occ) {
-        if (c0 != d || c1 != d)
-          return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": empty slots must carry (d, d)");
-        empty_seen = true;
-        if (b > 0 && b < n && hl[(size_t)b * chi + i] != 0.0)
-          return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": Lambda on an empty slot");
-        continue;
-      }
-      if (empty_seen) return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": occupied slot after an empty one");
-      if (c0 < 0 || c1 < 0 || c1 >= d) return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": charge out of range");
-      if (c0 < p0 || (c0 == p0 && c1 < p1))
-        return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": charges not sorted");
-      if (b > 0 && b < n && !(hl[(size_t)b * chi + i] > 0.0))
-        return fail(h, BSMPO_EINVAL, "bond " + std::to_string(b) + ": occupied slot with Lambda <= 0");
-      p0 = c0; p1 = c1;
-      h->cnt[(size_t)b * d * d + c0 * d + c1]++;
-    }
+    const int rc = validate_bond(h, b, hc + (size_t)b * chi * 2, hl + (size_t)b * chi, &h->cnt[(size_t)b * d * d]);
+    if (rc) return rc;
   }
   for (int b : {0, n})
     for (int i = 0; i < chi; ++i) hl[(size_t)b * chi + i] = hc[((size_t)b * chi + i) * 2] < d ? 1.0 : 0.0;
@@ -1687,6 +1696,59 @@ int bsmpo_store_state(bsmpo_ctx* h, void* gamma, double* lambda, int* charge) {
   if (lambda) CK(h, cudaMemcpyAsync(lambda, h->lam + chi, (size_t)(n - 1) * chi * sizeof(double), cudaMemcpyDeviceToDevice, st));
   if (charge) CK(h, cudaMemcpyAsync(charge, h->charge, (size_t)(n + 1) * chi * 2 * sizeof(int), cudaMemcpyDeviceToDevice, st));
   CK(h, cudaStreamSynchronize(st));
+  return BSMPO_OK;
+}
+
+int bsmpo_get_site(bsmpo_ctx* h, int site, void* gamma) {
+  if (!h || !h->loaded) return fail(h, BSMPO_EINVAL, "no state loaded");
+  if (!gamma || site < 0 || site >= h->n) return fail(h, BSMPO_EINVAL, "bad argument");
+  const size_t elems = (size_t)h->chi * h->chi;
+  CK(h, cudaMemcpyAsync(gamma, h->gamma + (size_t)site * elems, elems * sizeof(cplx), cudaMemcpyDeviceToDevice,
+                        h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return BSMPO_OK;
+}
+
+int bsmpo_put_site(bsmpo_ctx* h, int site, const void* gamma) {
+  if (!h || !h->loaded) return fail(h, BSMPO_EINVAL, "no state loaded");
+  if (!gamma || site < 0 || site >= h->n) return fail(h, BSMPO_EINVAL, "bad argument");
+  const size_t elems = (size_t)h->chi * h->chi;
+  CK(h, cudaMemcpyAsync(h->gamma + (size_t)site * elems, gamma, elems * sizeof(cplx), cudaMemcpyDeviceToDevice,
+                        h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return BSMPO_OK;
+}
+
+int bsmpo_get_bond(bsmpo_ctx* h, int bond, double* lambda, int* charge) {
+  if (!h || !h->loaded) return fail(h, BSMPO_EINVAL, "no state loaded");
+  if (!lambda || !charge || bond < 1 || bond >= h->n) return fail(h, BSMPO_EINVAL, "bad argument");
+  const int chi = h->chi;
+  CK(h, cudaMemcpyAsync(lambda, h->lam + (size_t)bond * chi, chi * sizeof(double), cudaMemcpyDeviceToDevice,
+                        h->stream));
+  CK(h, cudaMemcpyAsync(charge, h->charge + (size_t)bond * chi * 2, chi * 2 * sizeof(int),
+                        cudaMemcpyDeviceToDevice, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return BSMPO_OK;
+}
+
+int bsmpo_put_bond(bsmpo_ctx* h, int bond, const double* lambda, const int* charge) {
+  if (!h || !h->loaded) return fail(h, BSMPO_EINVAL, "no state loaded");
+  if (!lambda || !charge || bond < 1 || bond >= h->n) return fail(h, BSMPO_EINVAL, "bad argument");
+  const int chi = h->chi, dd = h->d * h->d;
+  // checked before it is written: a rejected bond leaves the state as it was
+  std::vector<double> hl(chi);
+  std::vector<int> hc((size_t)chi * 2), row(dd);
+  CK(h, cudaMemcpyAsync(hl.data(), lambda, chi * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaMemcpyAsync(hc.data(), charge, chi * 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  const int rc = validate_bond(h, bond, hc.data(), hl.data(), row.data());
+  if (rc) return rc;
+  CK(h, cudaMemcpyAsync(h->lam + (size_t)bond * chi, lambda, chi * sizeof(double), cudaMemcpyDeviceToDevice,
+                        h->stream));
+  CK(h, cudaMemcpyAsync(h->charge + (size_t)bond * chi * 2, charge, chi * 2 * sizeof(int),
+                        cudaMemcpyDeviceToDevice, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  std::copy(row.begin(), row.end(), h->cnt.begin() + (size_t)bond * dd);
   return BSMPO_OK;
 }
 

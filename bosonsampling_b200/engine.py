@@ -131,6 +131,43 @@ class MPOSimulator:
                                            ctypes.c_void_p(c.data_ptr())))
         return g, l, c
 
+    def get_site(self, site, out=None):
+        """Gamma[site] (complex128 chi x chi device tensor, ``out`` if given)."""
+        t = self.torch
+        if out is None:
+            out = t.empty((self.chi, self.chi), dtype=t.complex128, device=t.device("cuda", t.cuda.current_device()))
+        assert out.is_cuda and out.dtype == t.complex128 and out.is_contiguous() and out.numel() == self.chi ** 2
+        self._chk(self.L.bsmpo_get_site(self.h, int(site), ctypes.c_void_p(out.data_ptr())))
+        return out
+
+    def put_site(self, site, gamma):
+        t = self.torch
+        assert gamma.is_cuda and gamma.dtype == t.complex128 and gamma.is_contiguous() and gamma.numel() == self.chi ** 2
+        self._chk(self.L.bsmpo_put_site(self.h, int(site), ctypes.c_void_p(gamma.data_ptr())))
+
+    def get_bond(self, bond, lam=None, charge=None):
+        """(Lambda float64 [chi], charges int32 [chi, 2]) of bond 1..n-1, device tensors."""
+        t = self.torch
+        dev = t.device("cuda", t.cuda.current_device())
+        if lam is None:
+            lam = t.empty(self.chi, dtype=t.float64, device=dev)
+        if charge is None:
+            charge = t.empty((self.chi, 2), dtype=t.int32, device=dev)
+        self._check_bond_tensors(lam, charge)
+        self._chk(self.L.bsmpo_get_bond(self.h, int(bond), ctypes.c_void_p(lam.data_ptr()),
+                                        ctypes.c_void_p(charge.data_ptr())))
+        return lam, charge
+
+    def put_bond(self, bond, lam, charge):
+        self._check_bond_tensors(lam, charge)
+        self._chk(self.L.bsmpo_put_bond(self.h, int(bond), ctypes.c_void_p(lam.data_ptr()),
+                                        ctypes.c_void_p(charge.data_ptr())))
+
+    def _check_bond_tensors(self, lam, charge):
+        t = self.torch
+        assert lam.is_cuda and lam.dtype == t.float64 and lam.is_contiguous() and lam.numel() == self.chi
+        assert charge.is_cuda and charge.dtype == t.int32 and charge.is_contiguous() and charge.numel() == 2 * self.chi
+
     def init_product(self, rho_sites, total_photons=None, canonicalize=True):
         """Product-state MPO of the per-mode density matrices ``rho_sites`` (n of d x d),
         built on the device (``bsmpo_init_product``), then canonicalised."""

@@ -159,6 +159,19 @@ int bsmpo_set_cutoff(bsmpo_ctx* h, double cutoff);
 int bsmpo_load_state(bsmpo_ctx* h, const void* gamma, const double* lambda, const int* charge);
 int bsmpo_store_state(bsmpo_ctx* h, void* gamma, double* lambda, int* charge);
 
+/* One site or one bond of the loaded state, copied between the handle and device
+ * buffers of the caller: the units of the halo exchange of a circuit partitioned over
+ * several handles (ranks), replacing the per-site Gamma / Lambda / charge messages of
+ * src/fully_parallel/Full.py:70-103 and the per-request state shipping of
+ * src/beam_splitter_parallel/Full.py:149-166.  Site 0..n-1: Gamma[site], complex128
+ * chi x chi.  Bond 1..n-1 (between sites bond-1 and bond): Lambda double[chi] and
+ * charges int32[chi][2].  put_bond validates the bond as load_state does and leaves the
+ * state unchanged when it is rejected.  All return with the copy complete. */
+int bsmpo_get_site(bsmpo_ctx* h, int site, void* gamma);
+int bsmpo_put_site(bsmpo_ctx* h, int site, const void* gamma);
+int bsmpo_get_bond(bsmpo_ctx* h, int bond, double* lambda, int* charge);
+int bsmpo_put_bond(bsmpo_ctx* h, int bond, const double* lambda, const int* charge);
+
 /* Product-state MPO built on the device: the filling of the reference's Initialize
  * (src/MPO.py:56-109) for an arbitrary density matrix per mode.  rho: host
  * complex128 [n][d][d] (rho[site][ket occupation][bra occupation]).  Bond charges are
