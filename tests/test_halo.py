@@ -23,7 +23,7 @@ from bosonsampling_b200 import halo, interferometer  # noqa: E402
 
 
 def _replay(plan):
-    """Replays the plan on versioned items; returns the bytes-free transfer count."""
+    """Replays the plan on versioned items, asserting that every read and the gather see current versions."""
     n, world = plan.n, plan.world
     current = {}
     store = [dict() for _ in range(world)]
@@ -163,7 +163,7 @@ def test_two_gloo_ranks_reproduce_the_single_process_circuit():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         port = s.getsockname()[1]
-    out = mp.Manager().dict()
+    out = mp.get_context("spawn").Manager().dict()
     mp.start_processes(_rank_main, args=(world, port, out), nprocs=world, start_method="spawn", join=True)
     ref = _single_process()
     g, lam, chg = out["state"]

@@ -33,7 +33,7 @@ def _rank_main(rank, world, port, out):
 
 def test_two_replicas_time_is_the_slowest_rank():
     world, port = 2, _free_port()
-    out = mp.Manager().dict()
+    out = mp.get_context("spawn").Manager().dict()
     mp.start_processes(_rank_main, args=(world, port, out), nprocs=world, start_method="spawn", join=True)
     for r in range(world):
         t, rate = out[r]
