@@ -71,10 +71,13 @@ def parse():
     p.add_argument("--also", default="tf32x3",
                    help="comma-separated further precision forms timed on the same layers and "
                         "checked over the whole circuit ('' for none)")
-    p.add_argument("--batch", type=int, default=16,
+    p.add_argument("--batch", type=int, default=64,
                    help="independent circuits of the batched workload (N in [16, 48], eta in "
                         "[0.2, 0.8], d=4, chi in {128, 256, 512}) run side by side and one by one "
                         "(0: skip)")
+    p.add_argument("--batch-conc", default="4,8",
+                   help="comma-separated numbers of circuits run side by side in the batched form "
+                        "(the fastest is reported)")
     p.add_argument("--no-grad", action="store_true",
                    help="skip the differentiation form (N=24, d=4, chi=256 gradients of a marginal "
                         "loss, checked against central finite differences)")
@@ -596,7 +599,7 @@ def main():
         n_up = sum(len(sp["mesh"]) for sp in specs)
         engine.run_batch(specs[:2], concurrency=2, precision=args.precision)   # warm-up
         best = {}
-        for conc, wk in ((1, 8), (4, 4), (8, 4)):
+        for conc, wk in [(1, 8)] + [(int(c), 4) for c in args.batch_conc.split(",") if int(c) > 1]:
             tm = {}
             engine.run_batch(specs, concurrency=conc, precision=args.precision, workers=wk, timing=tm)
             best[conc] = tm["seconds"]
