@@ -59,6 +59,21 @@ def test_plan_delivers_every_read_and_gathers_on_root(n, world):
         assert all(not tr for tr in plan.transfers) and not plan.gather
 
 
+def test_other_root_and_custom_blocks():
+    n = 10
+    _, bs, _ = interferometer.circuit(n, 5)
+    layers = halo.layers_of(bs)
+    for owner, root in (([0, 0, 1, 1, 1, 2, 2, 2, 2], 2), ([1] * 4 + [0] * 5, 1), ([0] * 9, 0)):
+        plan = halo.HaloPlan(n, layers, 3, owner=owner, root=root)
+        _replay(plan)
+        ran = [sum(len(plan.local_layer(l, r)[0]) for l in range(len(layers))) for r in range(3)]
+        assert sum(ran) == len(bs)
+    # everything on one rank of three: nothing moves but the gather to another root
+    plan = halo.HaloPlan(n, layers, 3, owner=[0] * 9, root=2)
+    assert all(not tr for tr in plan.transfers)
+    assert plan.gather and all(src == 0 and dst == 2 for _, src, dst in plan.gather)
+
+
 def test_brick_wall_exchange_is_one_site_and_one_bond_per_boundary():
     n, world, chi = 16, 4, 64
     _, bs, _ = interferometer.circuit(n, 7)
