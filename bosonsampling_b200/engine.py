@@ -354,14 +354,22 @@ def batch_circuits(n_circuits=64, seed=1004, chis=(128, 256, 512), d=4):
     return specs
 
 
-def run_batch(specs, concurrency=8, precision="fp64-gram", workers=4, timing=None):
+def batch_cost(spec):
+    """Relative work of a circuit for ordering a batch: beam splitters x chi^3 (the
+    per-sector eigen/SVD work grows with the cube of the sector sizes, which chi caps)."""
+    return len(spec["mesh"]) * float(spec["chi"]) ** 3
+
+
+def run_batch(specs, concurrency=8, precision="fp64-gram", workers=4, timing=None, largest_first=False):
     """Runs independent circuits (``batch_circuits`` entries) side by side on the current
     device: ``concurrency`` circuits at a time, each on its own handle, host thread and
     stream (the library's calls release the GIL), each handle overlapping its own updates
     on ``workers`` streams.  Handles are created and initialised first and released last,
     outside the concurrent phase (allocating or freeing device memory synchronises the
-    whole device).  Returns ``[(trace, marginals)]`` in input order; every circuit
-    computes exactly what it computes alone.  ``timing`` (a dict), if given, receives the
+    whole device).  ``largest_first`` starts the circuits in decreasing ``batch_cost``
+    (longest-first list scheduling: the batch does not end on one large circuit running
+    alone).  Returns ``[(trace, marginals)]`` in input order; every circuit computes
+    exactly what it computes alone.  ``timing`` (a dict), if given, receives the
     wall-clock seconds of the concurrent phase (the meshes, phases and observables)."""
     import time
     from concurrent.futures import ThreadPoolExecutor
@@ -390,13 +398,16 @@ def run_batch(specs, concurrency=8, precision="fp64-gram", workers=4, timing=Non
                 sim.apply_phases(sp["phases"])
                 out[i] = sim.observables()
 
+        order = list(range(len(specs)))
+        if largest_first:
+            order.sort(key=lambda i: -batch_cost(specs[i]))
         t0 = time.perf_counter()
         if concurrency <= 1:
-            for i in range(len(specs)):
+            for i in order:
                 one(i)
         else:
             with ThreadPoolExecutor(max_workers=concurrency) as ex:
-                list(ex.map(one, range(len(specs))))
+                list(ex.map(one, order))
         torch.cuda.synchronize()
         if timing is not None:
             timing["seconds"] = time.perf_counter() - t0

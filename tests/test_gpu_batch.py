@@ -25,7 +25,8 @@ def test_batch_equals_one_by_one(precision):
                   mesh=[b for b in sp["mesh"] if b[1] < n - 1 and b[0] < n], phases=sp["phases"][:n])
     seq = engine.run_batch(specs, concurrency=1, precision=precision, workers=2)
     par = engine.run_batch(specs, concurrency=4, precision=precision, workers=2)
-    for (t1, p1), (t2, p2) in zip(seq, par):
-        assert t1 == t2
-        assert np.array_equal(p1, p2)
+    lpt = engine.run_batch(specs, concurrency=3, precision=precision, workers=2, largest_first=True)
+    for (t1, p1), (t2, p2), (t3, p3) in zip(seq, par, lpt):   # results in input order
+        assert t1 == t2 == t3
+        assert np.array_equal(p1, p2) and np.array_equal(p1, p3)
         assert abs(t1) > 0
