@@ -40,11 +40,19 @@ def _writes(m):
 
 def layers_of(mesh):
     """Group a mesh ``[(layer, mode, theta, phi), ...]`` into layers in order of first
-    appearance: ``[(modes, thetas, phis), ...]``."""
-    order, groups = [], defaultdict(list)
+    appearance: ``[(modes, thetas, phis), ...]``.  Raises ValueError where the grouping
+    would move a beam splitter before an earlier one on a shared site (the grouped
+    circuit would differ from the mesh applied in its order)."""
+    order, groups, pos, last = [], defaultdict(list), {}, {}
     for layer, mode, th, ph in mesh:
         if layer not in groups:
+            pos[layer] = len(order)
             order.append(layer)
+        g = pos[layer]
+        for site in (int(mode), int(mode) + 1):
+            if last.get(site, -1) > g:
+                raise ValueError(f"layer {layer}: mode {mode} follows a later layer's beam splitter on site {site}")
+            last[site] = g
         groups[layer].append((int(mode), float(th), float(ph)))
     out = []
     for layer in order:

@@ -99,6 +99,10 @@ def test_balanced_blocks_and_bad_layers():
         halo.HaloPlan(8, [([7], [0.1], [0.0])], 2)                # mode out of range
     with pytest.raises(ValueError):
         halo.HaloPlan(8, layers, 2, owner=[0] * 6)                # wrong length
+    # grouping by layer must not reorder beam splitters that share a site
+    with pytest.raises(ValueError):
+        halo.layers_of([(0, 0, 0.1, 0.0), (1, 1, 0.1, 0.0), (0, 2, 0.1, 0.0)])   # site 2: layer 1 then layer 0
+    assert len(halo.layers_of([(0, 0, 0.1, 0.0), (1, 1, 0.1, 0.0), (0, 3, 0.1, 0.0)])) == 2   # site-disjoint: fine
 
 
 class OracleSites:
