@@ -347,18 +347,37 @@ def run_reference(args):
 TRIDIAG_TRAFFIC = 2941184   # 2.836 MB read + 0.105 MB written
 
 
-def roofline(args, mine, kernel, fp64_peak, hbm_peak):
+def measured_peaks(path=os.path.join(ROOT, "MEASURED_PEAKS.json")):
+    """The pool's measured peaks (copy bandwidth ``hbm_gbs``, bf16 GEMM), or None."""
+    try:
+        with open(path) as f:
+            peaks = json.load(f)
+        return peaks if isinstance(peaks, dict) else None
+    except (OSError, ValueError):
+        return None
+
+
+def roofline(args, mine, kernel, fp64_peak, hbm_peak, peaks=None):
     """The dominant kernel's roofline.  Gram route: the Householder tridiagonalisation
     (tridiag_kernel, 66-71% of the update's kernel time), whose fused passes stream the
     trailing matrix once per step (read + write, 32 B per complex entry): achieved
-    bytes / device time of the phase, one worker, against the copy bandwidth measured in
-    this run.  Plain path: the Jacobi rounds' FP64 flops against measured DGEMM."""
+    bytes / device time of the phase, one worker, against the pool's measured copy
+    bandwidth (``peaks["hbm_gbs"]``), or the copy bandwidth measured in this run when
+    that is absent (both reported).  Plain path: the Jacobi rounds' FP64 flops against
+    DGEMM measured in this run (the pool's file holds no FP64 figure)."""
     if kernel is not None and kernel["ms"] > 0:
         achieved = kernel["bytes"] / (kernel["ms"] / 1e3) / 1e9
+        pool = float(peaks["hbm_gbs"]) if peaks and peaks.get("hbm_gbs") else None
+        peak = pool if pool else hbm_peak
         return {"kernel": "tridiag_kernel (Householder tridiagonalisation, four forked size-class launches)",
-                "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak if hbm_peak else None,
-                "peak_source": "copy bandwidth measured in this run (torch copy of 1 GiB, best of 10)",
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if peak else None,
+                "frac_of": "measured",
+                "peak_source": ("MEASURED_PEAKS.json hbm_gbs: copy bandwidth measured on this pool's B200s"
+                                if pool else
+                                "copy bandwidth measured in this run (torch copy of 1 GiB, best of 10)"),
+                "peak_in_run": hbm_peak,
+                "frac_of_in_run": achieved / hbm_peak if hbm_peak else None,
                 "achieved_over": "the phase's device time (CUDA events), one worker, one layer (%d phases)"
                                  % kernel["phases"],
                 "bytes": kernel["bytes"], "ms": kernel["ms"],
@@ -367,6 +386,7 @@ def roofline(args, mine, kernel, fp64_peak, hbm_peak):
     achieved = mine["svd_flops"] / mine["seconds"] / 1e12 if mine["seconds"] > 0 else None
     return {"kernel": SVD_KERNELS[args.precision], "bound": "tensor", "achieved": achieved, "peak": fp64_peak,
             "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if achieved and fp64_peak else None,
+            "frac_of": "measured",
             "peak_source": "FP64 DGEMM measured in this run (torch.matmul 8192^3, best of 5)",
             "achieved_over": "timed region (device time); the SVD phases of concurrent updates overlap",
             "traffic": None}
@@ -731,7 +751,7 @@ def main():
             "gpu_launches": int(mine["launches"]),
             "svd_routes": mine["routes"],
             "workspace_grows_in_timed_region": mine["workspace_grows"],
-            "roofline": roofline(args, mine, kernel, fp64_peak, hbm_peak),
+            "roofline": roofline(args, mine, kernel, fp64_peak, hbm_peak, measured_peaks()),
             "precision_forms": {form: {
                 "value": r["value"], "unit": "BS-updates/s", "speedup_vs_plain": (r["value"] / plain["value"]) if plain else None,
                 "prob_err_after_timed_layers": (float(np.abs(r["P"] - plain["P"]).max() / abs(plain["trace"]))
